@@ -1,0 +1,206 @@
+"""ORACLE bindings (test infrastructure only): ctypes access to the C restatement and a runner
+for the reference harness ``_ref/ref_dump``."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_libs: Dict[str, C.CDLL] = {}
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the restatement (always) and the reference harness (when its sources exist)."""
+    targets = ["restate"]
+    if os.path.isdir(os.environ.get("REFSRC", "/root/reference/src")):
+        targets.append("ref")
+    subprocess.run(["make", "-C", HERE, "-j8"] + targets, check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+
+
+def _lib(prec: str) -> C.CDLL:
+    if prec in _libs:
+        return _libs[prec]
+    path = os.path.join(BUILD_DIR, f"liboracle_{prec}.so")
+    lib = C.CDLL(path)
+    real = _f32p if prec == "f32" else _f64p
+    lib.orc_create.restype = C.c_void_p
+    lib.orc_create.argtypes = [C.c_int, C.c_int, C.c_double, _i32p, _f32p, _i32p, _i32p, _i32p, C.c_int, C.c_int, _i32p]
+    lib.orc_destroy.argtypes = [C.c_void_p]
+    lib.orc_rebuild.argtypes = [C.c_void_p, _f32p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
+    lib.orc_list_size.restype = C.c_long
+    lib.orc_list_size.argtypes = [C.c_void_p]
+    lib.orc_nghost.argtypes = [C.c_void_p]
+    lib.orc_num_gx.argtypes = [C.c_void_p]
+    lib.orc_get_list.argtypes = [C.c_void_p, _i32p]
+    lib.orc_get_sorted.argtypes = [C.c_void_p, _i32p, _i32p, _f64p]
+    lib.orc_pair_forces.argtypes = [C.c_void_p, _f32p, _f32p, C.c_int, C.c_double, _f64p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.orc_bonded.argtypes = [C.c_void_p, C.c_int, _i32p, _f32p, C.c_int, _i32p, _f32p, C.c_int, _i32p, _f32p,
+                               _f64p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.orc_gr_counts.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_double, _i64p, C.POINTER(C.c_int)]
+    lib.orc_nnp_tbl.argtypes = [C.c_void_p, C.c_double, C.c_int, _f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, _f32p,
+                                _f64p, _f64p, _f64p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.orc_nnp_emb.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, _f32p, C.c_int, C.c_int, _f32p,
+                                _f64p, _f64p, _f64p, _f64p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.orc_nnp_tables.argtypes = [C.c_int, C.c_double, C.c_int, _f32p, _f32p, _f32p, _f32p, real, real, real, real]
+    lib.orc_sq.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p]
+    _libs[prec] = lib
+    return lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, np.int32)
+
+
+class Restated:
+    """One system in the C restatement (``prec`` = "f32" follows the reference's float
+    arithmetic, "f64" is the FP64 oracle)."""
+
+    def __init__(self, sysm, prec: str = "f64"):
+        self.lib = _lib(prec)
+        self.sysm = sysm
+        mol_id, intra = sysm.mol_id_intra()
+        nmax = max(m.n_atom for m in sysm.moltypes)
+        spec = np.zeros((len(sysm.moltypes), nmax, nmax), np.int32)
+        for k, m in enumerate(sysm.moltypes):
+            spec[k, :m.n_atom, :m.n_atom] = m.special()
+        amt = sysm.mol_type[mol_id]
+        self.h = self.lib.orc_create(sysm.natom, sysm.ntype, float(sysm.bl), _i32(sysm.typ), _f32(sysm.q), _i32(mol_id),
+                                     _i32(intra), _i32(amt), len(sysm.moltypes), nmax, spec.ravel())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def rebuild(self, x, cutoff, skin, comm, cap=2048, max_nbin=126) -> int:
+        return self.lib.orc_rebuild(self.h, _f32(x).ravel(), cutoff, skin, comm, cap, max_nbin)
+
+    @property
+    def nghost(self) -> int:
+        return self.lib.orc_nghost(self.h)
+
+    def list_records(self) -> np.ndarray:
+        n = self.lib.orc_list_size(self.h)
+        rec = np.zeros(4 * n, np.int32)
+        self.lib.orc_get_list(self.h, rec)
+        return rec.reshape(-1, 4)
+
+    def pair_forces(self, F, U, cutoff):
+        """F, U: [npair, nbin+1] float tables (loadPotential layout)."""
+        F = _f32(F); U = _f32(U)
+        f = np.zeros(self.sysm.natom * 3)
+        e, w = C.c_double(0), C.c_double(0)
+        self.lib.orc_pair_forces(self.h, F.ravel(), U.ravel(), F.shape[1] - 1, cutoff, f, C.byref(e), C.byref(w))
+        return f.reshape(-1, 3), e.value, w.value
+
+    def bonded(self, bcoef, acoef, dcoef):
+        b, a, d = self.sysm.topology()
+        f = np.zeros(self.sysm.natom * 3)
+        e, w = C.c_double(0), C.c_double(0)
+        self.lib.orc_bonded(self.h, len(b), _i32(b).ravel(), _f32(bcoef).ravel(), len(a), _i32(a).ravel(),
+                            _f32(acoef).ravel(), len(d), _i32(d).ravel(), _f32(dcoef).ravel(), f, C.byref(e), C.byref(w))
+        return f.reshape(-1, 3), e.value, w.value
+
+    def gr_counts(self, gr_cutoff, skin, nbin_inner, r_inner):
+        dr = np.float32(r_inner) / np.float32(nbin_inner)
+        nmax = int(np.float32(gr_cutoff) * (np.float32(nbin_inner) / np.float32(r_inner))) + 2
+        cnt = np.zeros(self.sysm.npair * nmax, np.int64)
+        nb = C.c_int(0)
+        rc = self.lib.orc_gr_counts(self.h, gr_cutoff, skin, nbin_inner, r_inner, cnt, C.byref(nb))
+        assert rc == 0
+        return cnt[: self.sysm.npair * nb.value].reshape(self.sysm.npair, nb.value)
+
+    def nnp_tbl(self, cutoff, nbin, coef_p, coef_w, coef_d, coef_r, h1, h2, fitw):
+        n = self.sysm.natom
+        G = np.zeros(n * 20); dG = np.zeros(n * 20); f = np.zeros(n * 3)
+        ep, en, w = C.c_double(0), C.c_double(0), C.c_double(0)
+        self.lib.orc_nnp_tbl(self.h, cutoff, nbin, _f32(coef_p).ravel(), _f32(coef_w).ravel(), _f32(coef_d).ravel(),
+                             _f32(coef_r).ravel(), h1, h2, _f32(fitw).ravel(), G, dG, f, C.byref(ep), C.byref(en), C.byref(w))
+        return dict(G=G.reshape(n, 20), dEdG=dG.reshape(n, 20), f=f.reshape(n, 3), e_pair=ep.value, e_net=en.value, vir=w.value)
+
+    def nnp_emb(self, cutoff, e1, e2, embw, h1, h2, fitw):
+        n = self.sysm.natom
+        din = 4 * e2
+        G = np.zeros(n * din); dG = np.zeros(n * din); ea = np.zeros(n); f = np.zeros(n * 3)
+        en, w = C.c_double(0), C.c_double(0)
+        self.lib.orc_nnp_emb(self.h, cutoff, e1, e2, _f32(embw).ravel(), h1, h2, _f32(fitw).ravel(), G, dG, ea, f,
+                             C.byref(en), C.byref(w))
+        return dict(G=G.reshape(n, din), dEdG=dG.reshape(n, din), e_atom=ea, f=f.reshape(n, 3), e_net=en.value, vir=w.value)
+
+
+def sq(natom, bl, gr, dr, nq, qmax, prec="f64"):
+    gr = np.ascontiguousarray(gr, np.float64)
+    npair, nbin = gr.shape
+    out = np.zeros(npair * nq); qq = np.zeros(nq)
+    _lib(prec).orc_sq(natom, bl, nbin, dr, nq, qmax, npair, gr.ravel(), out, qq)
+    return out.reshape(npair, nq), qq
+
+
+# ----------------------------------------------------------------------------------------------
+# reference harness
+# ----------------------------------------------------------------------------------------------
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "ref_dump"))
+
+
+def run_ref_dump(cfg: Dict[str, str], workdir: str, fast: bool = False, env: Optional[dict] = None,
+                 timeout: float = 600) -> Dict[str, np.ndarray]:
+    """Write ``cfg`` (key -> value text) and run the reference harness; returns its arrays."""
+    os.makedirs(workdir, exist_ok=True)
+    cfg = dict(cfg)
+    cfg.setdefault("out", workdir)
+    path = os.path.join(workdir, "ref.cfg")
+    with open(path, "w") as f:
+        for k, v in cfg.items():
+            if isinstance(v, list):
+                for item in v:
+                    f.write(f"{k} {item}\n")
+            else:
+                f.write(f"{k} {v}\n")
+    exe = os.path.join(REF_DIR, "ref_dump_fast" if fast else "ref_dump")
+    subprocess.run([exe, path], check=True, cwd=workdir, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   env=env, timeout=timeout)
+    return read_ref_dump(workdir)
+
+
+def read_ref_dump(d: str) -> Dict[str, np.ndarray]:
+    out: Dict[str, np.ndarray] = {}
+    info = {}
+    with open(os.path.join(d, "info.txt")) as f:
+        for line in f:
+            k, v = line.split()
+            info[k] = float(v) if "." in v else int(v)
+    out["info"] = info
+    recs = []
+    for t in range(int(info["threads"])):
+        p = os.path.join(d, f"fulllist_t{t}.i32")
+        if os.path.exists(p):
+            recs.append(np.fromfile(p, np.int32).reshape(-1, 4))
+    if recs:
+        out["fulllist"] = np.concatenate(recs)
+    for name, dt in [("force.f32", np.float32), ("f.f32", np.float32), ("x.f32", np.float32), ("v.f32", np.float32),
+                     ("f_classical.f32", np.float32), ("desc.f32", np.float32), ("dedg.f32", np.float32),
+                     ("gr_counts.i64", np.int64), ("gr_inner_counts.i64", np.int64), ("gr.f32", np.float32),
+                     ("sq.f32", np.float32), ("qq.f32", np.float32), ("rr.f32", np.float32), ("log_e.f64", np.float64),
+                     ("log_w.f64", np.float64), ("log_k.f64", np.float64), ("log_enn.f64", np.float64)]:
+        p = os.path.join(d, name)
+        if os.path.exists(p):
+            out[name.split(".")[0]] = np.fromfile(p, dt)
+    return out
