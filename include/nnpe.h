@@ -1,0 +1,188 @@
+/* nnpe.h — C ABI of the B200 short-range force step (libnnpe.so).
+ *
+ * One context (nnpe_ctx) owns one periodic system resident in HBM: cell-sorted atoms, explicit
+ * periodic images ("ghosts"), the Verlet neighbour list, tables, descriptors and accumulators.
+ * Plain pointers and sizes only; host arrays are in atom-id order (the order of the
+ * configuration file), which is how the reference's ENVIRON::atom_id indexes results.
+ *
+ * Every call returns 0 on success or an NNPE_E* code; nnpe_last_error() gives the message.
+ * The reference ends the process on every such condition (END_PROGRAM, util.cpp:117-124); the
+ * C++ adapter in nnpe.hpp maps a non-zero status back to that behaviour.
+ *
+ * The "replaces" notes cite the reference member each entry point stands in for
+ * (paths within NNPEngine's src/).
+ */
+#ifndef NNPE_H
+#define NNPE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nnpe_ctx nnpe_ctx;
+
+enum {
+  NNPE_OK = 0,
+  NNPE_EARG = 1,       /* invalid argument or call order */
+  NNPE_ECUDA = 2,      /* CUDA runtime error */
+  NNPE_EOVERFLOW = 3,  /* a capacity was exceeded (list, ghosts, cell, stencil) */
+  NNPE_EFILE = 4,      /* input file missing or malformed */
+  NNPE_ERANGE = 5,     /* an atom left the cell grid */
+  NNPE_ETIMEOUT = 6    /* a bounded device wait gave up */
+};
+
+/* Device error bits accumulated by kernels (nnpe_device_errors). */
+enum {
+  NNPE_DEV_LIST_OVERFLOW = 1,   /* "nei_list overflow", neighlist.cpp:327 */
+  NNPE_DEV_GHOST_OVERFLOW = 2,  /* "ghost overflow", environ.cpp:440 */
+  NNPE_DEV_CELL_RANGE = 4,      /* an atom or image outside the grid (CHECK_BINNING, environ.cpp:245-259) */
+  NNPE_DEV_CELL_OVERFLOW = 8,   /* a cell holds more atoms than the in-cell sort supports */
+  NNPE_DEV_NAN = 16
+};
+
+/* Per-log-step record of the step loop (run.cpp:376-392 prints the same quantities). */
+typedef struct nnpe_thermo {
+  int step;
+  int nbuild;         /* NEIGHLIST::nbuild */
+  double erg;         /* potential energy [kcal/mol] (FP64 reduction) */
+  double virial;      /* sum of fpair*rsq [kcal/mol] */
+  double ekin;        /* kinetic energy [kcal/mol] before the thermostat */
+  double temperature; /* ekin/natom*ek_T [K] */
+  double pressure;    /* (virial+2 ekin)/3 * ev_GPa / BL^3 [GPa] */
+  double erg_nnp;     /* network part of erg */
+} nnpe_thermo;
+
+/* ---- context -------------------------------------------------------------------------- */
+int nnpe_create(int device, nnpe_ctx** out);
+void nnpe_destroy(nnpe_ctx* ctx);
+const char* nnpe_last_error(const nnpe_ctx* ctx);
+/* Raw device error bits since the last call to this function (then cleared). */
+int nnpe_device_errors(nnpe_ctx* ctx, int* bits);
+/* Stream all work of this context is issued on (cudaStream_t as void*). */
+void* nnpe_stream(nnpe_ctx* ctx);
+
+/* ---- system (replaces ENVIRON::initialize, environ.cpp:22-141; MOLECULE::from_file,
+ *      molecule.cpp:25-134) ------------------------------------------------------------- */
+/* special: [nmoltype][nmax][nmax] special class per intra-molecule atom pair (0..3);
+ * mol_rep: per molecule, the atom id of its representative (intra id 0). */
+int nnpe_set_system(nnpe_ctx* ctx, int natom, int ntype, double bl, const int* typ, const float* mass,
+                    const float* q, const float* x, const int* mol_id, const int* intra_id,
+                    const int* atom_moltype, int nmoltype, int nmax, const int* special);
+/* Parses the reference's initial-configuration file and its molecule files. */
+int nnpe_load_system_file(nnpe_ctx* ctx, const char* init_file);
+int nnpe_natom(const nnpe_ctx* ctx);
+int nnpe_npair(const nnpe_ctx* ctx);
+/* Positions/velocities in atom-id order, float [natom*3]; replace the state in place. */
+int nnpe_set_positions(nnpe_ctx* ctx, const float* x);
+int nnpe_set_velocities(nnpe_ctx* ctx, const float* v);
+
+/* ---- cutoffs, grid and stencils (replaces ENVIRON::init_grid environ.cpp:143-155,
+ *      LOCAL::set_ghost_lim environ.h:142, NEIGHLIST::build_bin_list neighlist.cpp:35-168,
+ *      NEIGHLIST ctor neighlist.cpp:13-33; wiring as run.cpp:72-82) ----------------------- */
+/* neigh_cap: per-atom list capacity (NEIGH_SZ, run.h:2). nnp_cutoff > 0 adds the short
+ * descriptor cutoff of a network term sharing the same list. */
+int nnpe_setup(nnpe_ctx* ctx, double pair_cutoff, double skin, double gr_cutoff, int neigh_cap);
+
+/* ---- LJTableCoulDSF (pair.h:30-54) ---------------------------------------------------- */
+/* Tables [npair][nbin+1] of F(r)/r and U(r) at r=(i+.5)dr, dr=cutoff/nbin, last column 0
+ * (replaces loadPotential, pair.cpp:197-263; the device copy is the `force/potential` pair). */
+int nnpe_pair_set_table(nnpe_ctx* ctx, int nbin, const float* force, const float* potential);
+int nnpe_pair_load_table(nnpe_ctx* ctx, int nbin, const char* potfile);
+int nnpe_pair_get_table(nnpe_ctx* ctx, float* force, float* potential);
+int nnpe_pair_enable(nnpe_ctx* ctx, int on);
+
+/* ---- bonded terms (BOND/ANGLE/DIHEDRAL, bond.h:6-21, angle.h:6-21, dihedral.h:4-17) ----
+ * Terms in atom ids (as autoGenerate expands them, bond.cpp:66-86); coefficients in the
+ * stored form of setParam: bond (b0, 2a, b, 2c), angle (cos t0, 2a, b, 2c), dihedral
+ * (c0-c2, c1-3c3, 4c2, 12c3). */
+/* setParam in the reference's float arithmetic: the stored forms above from raw parameters
+ * (BOND::setParam bond.cpp:48-55, ANGLE::setParam angle.cpp:184-191 with theta0 in degrees,
+ * DIHEDRAL::setParam dihedral.cpp:340-348). out: 4 floats. */
+int nnpe_bond_coef(double b0, double ka, double kb, double kc, float* out);
+int nnpe_angle_coef(double theta0, double ka, double kb, double kc, float* out);
+int nnpe_dihedral_coef(double c0, double c1, double c2, double c3, float* out);
+/* BOND/ANGLE/DIHEDRAL::autoGenerate (bond.cpp:66-103): the terms of every molecule read by
+ * nnpe_load_system_file, with ntyp coefficient rows each in the stored form. */
+int nnpe_bonded_autogen(nnpe_ctx* ctx, int nbtyp, const float* bcoef, int natyp, const float* acoef, int ndtyp,
+                        const float* dcoef);
+int nnpe_bonded_set(nnpe_ctx* ctx, int nbond, const int* bonds, int nbtyp, const float* bcoef, int nangle,
+                    const int* angles, int natyp, const float* acoef, int ndih, const int* dihs, int ndtyp,
+                    const float* dcoef);
+
+/* ---- VERLET (verlet.h:4-22) and thermostat (run.cpp:348-373) --------------------------- */
+/* fp64_state = 1: positions/velocities advanced in FP64 (default); 0: the reference's float
+ * arithmetic, bit for bit. */
+int nnpe_verlet_setup(nnpe_ctx* ctx, double dt, int fp64_state);
+/* Number of steps the thermostat temperature ramp spans (total_steps of run.cpp:185). */
+int nnpe_set_total_steps(nnpe_ctx* ctx, int total_steps);
+/* thermostat: 0 none (NVE), 1 Andersen (re-draw `frac` of velocities, run.cpp:360-364),
+ * 2 CSVR (run.cpp:365-372). Temperature ramps from t_start to t_end over the run. */
+int nnpe_thermostat(nnpe_ctx* ctx, int kind, double t_start, double t_end, int interval, double frac,
+                    uint64_t seed);
+
+/* ---- the neighbour list (NEIGHLIST, neighlist.h:6-47) ---------------------------------- */
+/* Rebuild: refold_and_tag, sort, generate_ghost, tidyup_ghost, update_ghost_pos<true>,
+ * sort_ghost, update_ghost_and_info, build (run.cpp:249-276). */
+int nnpe_list_build(nnpe_ctx* ctx);
+/* NEIGHLIST::isvalid (neighlist.cpp:178-187), AND over all atoms. */
+int nnpe_list_isvalid(nnpe_ctx* ctx, int* valid);
+/* update_ghost_pos<false> (environ.cpp:488-522). */
+int nnpe_ghost_update(nnpe_ctx* ctx);
+/* Sizes: natom, nghost, total list entries, nbuild. */
+int nnpe_list_info(nnpe_ctx* ctx, int* nghost, int64_t* nentries, int* nbuild, int* num_gx);
+/* Full list as records (atom id i, atom id j, image code, special class); image code
+ * (sx+1)*9+(sy+1)*3+(sz+1) of the ghost shift, 13 for a real atom. cap = record capacity. */
+int nnpe_list_get(nnpe_ctx* ctx, int64_t cap, int* rec, int64_t* n);
+
+/* ---- forces (pair.cpp:289-419, bond/angle/dihedral compute, run.cpp:302-342) ------------
+ * Clears the forces and evaluates pair + bonded (+ network when loaded) at the current
+ * positions; erg/virial are FP64 device reductions (NULL to skip, i.e. ev=false). */
+int nnpe_compute_forces(nnpe_ctx* ctx, int ev, double* erg, double* virial);
+/* Force evaluation at host positions (atom-id order, float [natom*3]): the call a host-side
+ * run loop makes in place of clear_vector/bond/angle/dihedral/pair.compute (run.cpp:302-342),
+ * with the list check and rebuild of run.cpp:236-283 done on the device first. Writes the forces
+ * to f_host (atom-id order); erg/virial (FP64) when non-NULL. */
+int nnpe_force_step(nnpe_ctx* ctx, const float* x_host, float* f_host, double* erg, double* virial);
+/* Forces (kind 0) or accelerations after the last step (kind 1), atom-id order [natom*3]. */
+int nnpe_get_forces(nnpe_ctx* ctx, int kind, float* f);
+int nnpe_get_positions(nnpe_ctx* ctx, float* x);
+int nnpe_get_positions_f64(nnpe_ctx* ctx, double* x);
+int nnpe_get_velocities(nnpe_ctx* ctx, float* v);
+int nnpe_get_velocities_f64(nnpe_ctx* ctx, double* v);
+/* Per-atom energies of the last ev evaluation, atom-id order (FP64). */
+int nnpe_get_atom_energy(nnpe_ctx* ctx, double* e);
+
+/* ---- the step loop (classical, run.cpp:192-394; nnp_run, run.cpp:1087-1354) -----------
+ * Runs steps md_step=first..first+nsteps-1 of updateX, list check/rebuild, g(r) tally on
+ * gr_interval, forces, updateV, thermostat; records one nnpe_thermo per log_interval into
+ * log (capacity max_log, count in *nlog). The first call after setup performs the
+ * reference's initial updateX with -dt (run.cpp:193-227). */
+int nnpe_run(nnpe_ctx* ctx, int nsteps, int log_interval, nnpe_thermo* log, int max_log, int* nlog);
+/* Same loop with all device work of each step captured once in a CUDA graph and replayed;
+ * the rebuild decision stays on the device. */
+int nnpe_run_graph(nnpe_ctx* ctx, int nsteps, int log_interval, nnpe_thermo* log, int max_log, int* nlog);
+
+/* ---- profiling ------------------------------------------------------------------------
+ * Enqueue one kernel class without synchronising (for event timing): 0 pair force, 1 list
+ * rebuild, 2 bonded, 3 network term, 4 Verlet, 5 cell-based g(r), 6 list-based g(r). */
+int nnpe_profile_enqueue(nnpe_ctx* ctx, int which);
+/* Number of kernel launches in one plain MD step (the nodes of its CUDA graph). */
+int nnpe_launches_per_step(nnpe_ctx* ctx);
+
+/* ---- g(r) and S(q) (GR/SQ, grsq.h:8-38) -----------------------------------------------
+ * GR(nbin_inner, gr_cutoff, pair_cutoff) bins (grsq.cpp:28-80); SQ(nq, qmax) (grsq.cpp:258-288). */
+int nnpe_gr_setup(nnpe_ctx* ctx, int nbin_inner, int nq, double qmax, int gr_interval, int gr_interval_long);
+/* Tally the current configuration (inner=1: list-based to the pair cutoff, grsq.cpp:94-149;
+ * inner=0: cell-based to gr_cutoff, grsq.cpp:151-205) into fresh uint64 counts. */
+int nnpe_gr_tally(nnpe_ctx* ctx, int inner);
+int nnpe_gr_nbin(const nnpe_ctx* ctx, int inner);
+/* counts [npair][nbin] (uint64, exact); gr [npair][nbin] = counts*norm-1 in FP64
+ * (reduce_local grsq.cpp:207-219 with a double normaliser); sq [npair][nq] in FP64. */
+int nnpe_gr_get(nnpe_ctx* ctx, int inner, uint64_t* counts, double* gr);
+int nnpe_sq_compute(nnpe_ctx* ctx, int inner, double* sq, double* q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NNPE_H */

@@ -1,0 +1,412 @@
+// Pair forces (LJTableCoulDSF, pair.cpp:289-419) and bonded terms (bond.cpp:108-137,
+// angle.cpp:245-294, dihedral.cpp:403-460), plus the deterministic FP64 energy reduction.
+//
+// Compiled with -fmad=false: every float expression below evaluates in the order the reference
+// spells it, without contraction, so a pair's fpair is the reference's bit for bit; only the
+// summation order over neighbours differs (full list, warp gather instead of the half list).
+#include "internal.cuh"
+
+namespace {
+
+__constant__ float c_special_lj[4] = {1.f, 0.f, 0.f, 0.5f};
+__constant__ float c_special_coul[4] = {1.f, 0.f, 0.f, (float)(5 / 6.)};
+constexpr float kElectricK = 332.06371f;
+
+struct PairParams {
+  const float4* pos;
+  const uint32_t* list;
+  const int* ncount;
+  const int2* info;
+  const float2* table;
+  const int* pairtype;
+  float4* frc;
+  double* eatom;
+  double* watom;
+  int N, cap, ntype, nbin;
+  float cutoff, cutsq, r_dr, vc, fc;
+  bool accumulate;
+};
+
+// One warp per atom: lanes stride over the atom's list row (coalesced 128-byte reads), gather
+// neighbour positions, and reduce with shuffles; the warp writes the atom's force once (no
+// atomics, deterministic).
+template <bool EV>
+__global__ void __launch_bounds__(128) k_pair(PairParams p) {
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= p.N) return;
+  const float4 xi = p.pos[i];
+  const int ti = p.info[i].y & 0xFF;
+  const int* ptrow = p.pairtype + ti * p.ntype;
+  const uint32_t* row = p.list + (size_t)i * p.cap;
+  const int n = p.ncount[i];
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  double e = 0.0, w = 0.0;
+  for (int k = lane; k < n; k += 32) {
+    const uint32_t ent = __ldg(row + k);
+    const int j = (int)(ent & NNPE_J_MASK);
+    const float4 xj = __ldg(p.pos + j);
+    float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float rsq = dx * dx + dy * dy + dz * dz;
+    if (rsq < p.cutsq) {
+      const int tj = (ent >> 27) & 7, s = ent >> 30;
+      const float r = sqrtf(rsq);
+      float ipw1 = r * p.r_dr - 0.5F;
+      const int t1 = (int)ipw1;
+      const float ipw2 = ipw1 - (float)t1;
+      ipw1 = 1 - ipw2;
+      const float2* tab = p.table + (size_t)ptrow[tj] * (p.nbin + 1);
+      const float2 a = __ldg(tab + t1), b = __ldg(tab + t1 + 1);
+      float fpair = (a.x * ipw1 + b.x * ipw2) * c_special_lj[s];
+      const float qq = xi.w * xj.w * kElectricK;
+      fpair += qq * (1 / (r * rsq) + p.fc / r) * c_special_coul[s];
+      fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+      if (EV) {
+        const float u = (a.y * ipw1 + b.y * ipw2) * c_special_lj[s] +
+                        qq * (1 / r + p.vc + p.fc * (p.cutoff - r)) * c_special_coul[s];
+        e += 0.5 * (double)u;
+        w += 0.5 * (double)(fpair * rsq);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    if (EV) {
+      e += __shfl_xor_sync(0xffffffffu, e, o);
+      w += __shfl_xor_sync(0xffffffffu, w, o);
+    }
+  }
+  if (lane == 0) {
+    if (p.accumulate) {
+      float4 f = p.frc[i];
+      p.frc[i] = make_float4(f.x + fx, f.y + fy, f.z + fz, 0.f);
+    } else {
+      p.frc[i] = make_float4(fx, fy, fz, 0.f);
+    }
+    if (EV) {
+      p.eatom[i] = p.accumulate ? p.eatom[i] + e : e;
+      p.watom[i] = p.accumulate ? p.watom[i] + w : w;
+    }
+  }
+}
+
+__global__ void k_zero_forces(float4* frc, double* eatom, double* watom, int N) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  frc[i] = make_float4(0, 0, 0, 0);
+  eatom[i] = 0;
+  watom[i] = 0;
+}
+
+struct BondedParams {
+  const float4* pos;
+  const int* sorted_of_id;
+  const int* molshift;
+  const int* terms;        // per molecule [bond, angle, dih] starts
+  const int4* bond;
+  const int4* angle;
+  const int* dih;
+  const float4* bcoef;
+  const float4* acoef;
+  const float4* dcoef;
+  float4* frc;
+  double* emol;
+  double* wmol;
+  int nmol;
+  GridParams g;
+};
+
+// x_mol (environ.h:38-40): the real atom or the periodic image of it that lies within half a box
+// of its molecule's representative, recomputed as x + shift every step like the image itself.
+__device__ __forceinline__ float3 xmol(const BondedParams& p, int a, int* si) {
+  const int s = p.sorted_of_id[a];
+  *si = s;
+  const float4 x = p.pos[s];
+  float sh[3];
+  shift_of(p.g, p.molshift[a], sh);
+  return make_float3(x.x + sh[0], x.y + sh[1], x.z + sh[2]);
+}
+__device__ __forceinline__ void addf(float4* frc, int s, float fx, float fy, float fz) {
+  float4 f = frc[s];
+  frc[s] = make_float4(f.x + fx, f.y + fy, f.z + fz, f.w);
+}
+
+// One thread per molecule evaluates all of its bonded terms (molecules never share atoms, so
+// the read-modify-write of the atoms' forces is race free).
+template <bool EV>
+__global__ void k_bonded(BondedParams p) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= p.nmol) return;
+  float e = 0.f, w = 0.f;
+  const int b0 = p.terms[3 * m], b1 = p.terms[3 * m + 3];
+  for (int t = b0; t < b1; ++t) {
+    const int4 b = p.bond[t];
+    const float4 c = p.bcoef[b.x];
+    int si, sj;
+    const float3 xi = xmol(p, b.y, &si), xj = xmol(p, b.z, &sj);
+    float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    float rr = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float dr = rr - c.x;
+    const float bdr = c.z - dr;
+    const float ff = dr * (c.w + c.y * bdr * (bdr - dr)) / rr;
+    dx *= ff; dy *= ff; dz *= ff;
+    addf(p.frc, si, -dx, -dy, -dz);
+    addf(p.frc, sj, dx, dy, dz);
+    if (EV) {
+      e += 0.5F * (dr * dr) * (c.y * (bdr * bdr) + c.w);
+      w -= ff * rr * rr;
+    }
+  }
+  const int a0 = p.terms[3 * m + 1], a1 = p.terms[3 * m + 4];
+  for (int t = a0; t < a1; ++t) {
+    const int4 a = p.angle[t];
+    const float4 c = p.acoef[a.x];
+    int si, sj, sk;
+    const float3 xi = xmol(p, a.y, &si), xj = xmol(p, a.z, &sj), xk = xmol(p, a.w, &sk);
+    float dx1 = xi.x - xj.x, dy1 = xi.y - xj.y, dz1 = xi.z - xj.z;
+    float dx2 = xk.x - xj.x, dy2 = xk.y - xj.y, dz2 = xk.z - xj.z;
+    const float r_r1 = 1 / sqrtf(dx1 * dx1 + dy1 * dy1 + dz1 * dz1);
+    const float r_r2 = 1 / sqrtf(dx2 * dx2 + dy2 * dy2 + dz2 * dz2);
+    dx1 *= r_r1; dy1 *= r_r1; dz1 *= r_r1;
+    dx2 *= r_r2; dy2 *= r_r2; dz2 *= r_r2;
+    const float cq = dx1 * dx2 + dy1 * dy2 + dz1 * dz2;
+    const float dcq = cq - c.x;
+    const float b_dcq = c.z - dcq;
+    const float fe = dcq * (c.w + c.y * b_dcq * (b_dcq - dcq));
+    float ff = fe * r_r1;
+    float fx = ff * (cq * dx1 - dx2), fy = ff * (cq * dy1 - dy2), fz = ff * (cq * dz1 - dz2);
+    addf(p.frc, si, fx, fy, fz);
+    addf(p.frc, sj, -fx, -fy, -fz);
+    ff = fe * r_r2;
+    fx = ff * (dx1 - cq * dx2); fy = ff * (dy1 - cq * dy2); fz = ff * (dz1 - cq * dz2);
+    addf(p.frc, sk, -fx, -fy, -fz);
+    addf(p.frc, sj, fx, fy, fz);
+    if (EV) e += 0.5F * (dcq * dcq) * (c.y * (b_dcq * b_dcq) + c.w);
+  }
+  const int d0 = p.terms[3 * m + 2], d1 = p.terms[3 * m + 5];
+  for (int t = d0; t < d1; ++t) {
+    const int* d = p.dih + 5 * t;
+    const float4 c = p.dcoef[d[0]];
+    int si, sj, sk, sl;
+    const float3 xi = xmol(p, d[1], &si), xj = xmol(p, d[2], &sj), xk = xmol(p, d[3], &sk), xl = xmol(p, d[4], &sl);
+    float dx1 = xi.x - xj.x, dy1 = xi.y - xj.y, dz1 = xi.z - xj.z;
+    float dx2 = xk.x - xj.x, dy2 = xk.y - xj.y, dz2 = xk.z - xj.z;
+    float dx3 = xl.x - xk.x, dy3 = xl.y - xk.y, dz3 = xl.z - xk.z;
+    const float r_rsq2 = 1 / (dx2 * dx2 + dy2 * dy2 + dz2 * dz2);
+    const float dot12 = (dx1 * dx2 + dy1 * dy2 + dz1 * dz2) * r_rsq2;
+    const float dot32 = (dx3 * dx2 + dy3 * dy2 + dz3 * dz2) * r_rsq2;
+    dx1 -= dx2 * dot12; dy1 -= dy2 * dot12; dz1 -= dz2 * dot12;
+    dx3 -= dx2 * dot32; dy3 -= dy2 * dot32; dz3 -= dz2 * dot32;
+    float r_r1 = 1 / sqrtf(dx1 * dx1 + dy1 * dy1 + dz1 * dz1);
+    float r_r3 = 1 / sqrtf(dx3 * dx3 + dy3 * dy3 + dz3 * dz3);
+    dx1 *= r_r1; dy1 *= r_r1; dz1 *= r_r1;
+    dx3 *= r_r3; dy3 *= r_r3; dz3 *= r_r3;
+    const float cq = dx1 * dx3 + dy1 * dy3 + dz1 * dz3;
+    const float ff = (c.w * cq + c.z) * cq + c.y;
+    r_r1 *= ff; r_r3 *= ff;
+    const float f1x = r_r1 * (cq * dx1 - dx3), f1y = r_r1 * (cq * dy1 - dy3), f1z = r_r1 * (cq * dz1 - dz3);
+    const float f3x = r_r3 * (cq * dx3 - dx1), f3y = r_r3 * (cq * dy3 - dy1), f3z = r_r3 * (cq * dz3 - dz1);
+    const float f2x = f1x * dot12 + f3x * dot32, f2y = f1y * dot12 + f3y * dot32, f2z = f1z * dot12 + f3z * dot32;
+    addf(p.frc, si, f1x, f1y, f1z);
+    addf(p.frc, sl, f3x, f3y, f3z);
+    addf(p.frc, sj, f2x - f1x, f2y - f1y, f2z - f1z);
+    addf(p.frc, sk, -(f2x + f3x), -(f2y + f3y), -(f2z + f3z));
+    if (EV) e += ((c.w / 3 * cq + c.z / 2) * cq + c.y) * cq + c.x;
+  }
+  if (EV) {
+    p.emol[m] = e;
+    p.wmol[m] = w;
+  }
+}
+
+// Deterministic FP64 reduction of per-atom / per-molecule partials into d_red:
+// [0] pair+bonded energy, [1] virial, [2] kinetic energy, [3] network energy.
+__device__ double block_sum(double v, double* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] += sh[t + s];
+    __syncthreads();
+  }
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(1024) k_reduce(const double* eatom, const double* watom, const double* kin,
+                                                 const double* emol, const double* wmol, const double* enet, int N,
+                                                 int nmol, int nnet, bool with_kin, double* red, LogRec* log,
+                                                 int log_cap, int* ctrl, bool write_log) {
+  __shared__ double sh[1024];
+  const int t = threadIdx.x;
+  double e = 0, w = 0, k = 0, en = 0;
+  for (int i = t; i < N; i += blockDim.x) { e += eatom[i]; w += watom[i]; if (with_kin) k += kin[i]; }
+  for (int m = t; m < nmol; m += blockDim.x) { e += emol[m]; w += wmol[m]; }
+  for (int m = t; m < nnet; m += blockDim.x) en += enet[m];
+  e = block_sum(e, sh);
+  w = block_sum(w, sh);
+  k = block_sum(k, sh);
+  en = block_sum(en, sh);
+  if (t == 0) {
+    red[0] = e + en; red[1] = w; red[3] = en;
+    if (with_kin) red[2] = k;
+    if (write_log) {
+      const int slot = ctrl[CTRL_NLOG];
+      if (slot < log_cap) {
+        LogRec r;
+        r.erg = e + en; r.virial = w; r.ekin = with_kin ? k : red[2]; r.erg_nnp = en;
+        r.step = ctrl[CTRL_STEP]; r.nbuild = ctrl[CTRL_NBUILD]; r.pad0 = r.pad1 = 0;
+        log[slot] = r;
+      }
+      ctrl[CTRL_NLOG] = slot + 1;
+    }
+  }
+}
+
+}  // namespace
+
+const double* nnp_atom_energy_ptr(nnpe_ctx* c);   // nnp.cu
+
+int pair_enqueue(nnpe_ctx* c, bool ev) {
+  const int N = c->natom;
+  PairParams p;
+  p.pos = c->d_pos; p.list = c->d_list; p.ncount = c->d_ncount; p.info = c->d_info; p.table = c->d_table;
+  p.pairtype = c->d_pairtype; p.frc = c->d_frc; p.eatom = c->d_eatom; p.watom = c->d_watom;
+  p.N = N; p.cap = c->cap; p.ntype = c->ntype; p.nbin = c->nbin;
+  p.cutoff = c->pair_cutoff; p.cutsq = c->pair_cutoff * c->pair_cutoff;
+  p.r_dr = (float)c->nbin / c->pair_cutoff;   // LJTableCoulDSF ctor (pair.cpp:176-177)
+  p.vc = -1 / p.cutoff; p.fc = p.vc / p.cutoff;  // pair.cpp:191-193 (erfc disabled)
+  p.accumulate = false;
+  const int blocks = nblocks((long)N * 32, 128);
+  if (ev) k_pair<true><<<blocks, 128, 0, c->stream>>>(p);
+  else k_pair<false><<<blocks, 128, 0, c->stream>>>(p);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int bonded_enqueue(nnpe_ctx* c, bool ev) {
+  cudaStream_t st = c->stream;
+  if (c->d_mol_terms && (c->nbond + c->nangle + c->ndih) > 0) {
+    BondedParams b;
+    b.pos = c->d_pos; b.sorted_of_id = c->d_sorted_of_id; b.molshift = c->d_molshift; b.terms = c->d_mol_terms;
+    b.bond = c->d_bond; b.angle = c->d_angle; b.dih = c->d_dih; b.bcoef = c->d_bcoef; b.acoef = c->d_acoef;
+    b.dcoef = c->d_dcoef; b.frc = c->d_frc; b.emol = c->d_emol; b.wmol = c->d_wmol; b.nmol = c->nmol; b.g = c->grid;
+    if (ev) k_bonded<true><<<nblocks(c->nmol, 128), 128, 0, st>>>(b);
+    else k_bonded<false><<<nblocks(c->nmol, 128), 128, 0, st>>>(b);
+  } else if (ev) {
+    NNPE_CUDA(c, cudaMemsetAsync(c->d_emol, 0, sizeof(double) * c->nmol, st));
+    NNPE_CUDA(c, cudaMemsetAsync(c->d_wmol, 0, sizeof(double) * c->nmol, st));
+  }
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+// The force block: pair (writes the forces), network term (adds), bonded terms (add).
+int forces_enqueue(nnpe_ctx* c, bool ev) {
+  if (c->pair_on && c->d_table) {
+    if (int rc = pair_enqueue(c, ev)) return rc;
+  } else {
+    k_zero_forces<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_frc, c->d_eatom, c->d_watom, c->natom);
+  }
+  if (c->nnp)
+    if (int rc = nnp_forces_enqueue(c, ev)) return rc;
+  if (int rc = bonded_enqueue(c, ev)) return rc;
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int energy_reduce_enqueue(nnpe_ctx* c, int mode) {
+  // mode 0: energies only; 1: energies + kinetic into the log; 2: kinetic only (no log)
+  const double* enet = c->nnp ? nnp_atom_energy_ptr(c) : nullptr;
+  const int nnet = enet ? c->natom : 0;
+  const bool bonded = c->d_mol_terms && (c->nbond + c->nangle + c->ndih) > 0;
+  k_reduce<<<1, 1024, 0, c->stream>>>(c->d_eatom, c->d_watom, c->d_kin, c->d_emol, c->d_wmol, enet, c->natom,
+                                      bonded || mode >= 0 ? c->nmol : 0, nnet, mode >= 1, c->d_red, c->d_log,
+                                      c->log_cap, c->d_ctrl, mode == 1);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int nnpe_sync_errors(nnpe_ctx* c);
+int check_valid_enqueue(nnpe_ctx* c);
+
+namespace {
+// positions in atom-id order (host layout) -> sorted master/FP32 coordinates
+__global__ void k_scatter_positions(const float* __restrict__ x, const int* __restrict__ aid, double4* __restrict__ xd,
+                                    float4* __restrict__ pos, int N) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const int a = aid[k];
+  const float px = x[3 * a], py = x[3 * a + 1], pz = x[3 * a + 2];
+  xd[k] = make_double4(px, py, pz, 0);
+  pos[k] = make_float4(px, py, pz, pos[k].w);
+}
+// sorted forces -> atom-id order
+__global__ void k_gather_forces(const float4* __restrict__ frc, const int* __restrict__ aid, float* __restrict__ f, int N) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const int a = aid[k];
+  const float4 v = frc[k];
+  f[3 * a] = v.x; f[3 * a + 1] = v.y; f[3 * a + 2] = v.z;
+}
+__global__ void k_qm_to_pos(const float2* __restrict__ qm, float4* __restrict__ pos, int N) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < N) pos[k].w = qm[k].x;
+}
+}  // namespace
+
+// Force evaluation at caller-owned host positions: the drop-in call a host-side run loop makes
+// (positions in, forces and energy out, in atom-id order). The list is checked and rebuilt on the
+// device as needed (run.cpp:236-283), then the force block runs (run.cpp:302-342).
+extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial) {
+  if (!c || !c->have_setup || !x_host || !f_host) return nnpe_fail(c, NNPE_EARG, "nnpe_force_step");
+  cudaSetDevice(c->device);
+  const int N = c->natom;
+  if (!c->d_xstage) {
+    NNPE_CUDA(c, cudaMalloc(&c->d_xstage, sizeof(float) * 3 * N));
+    NNPE_CUDA(c, cudaMalloc(&c->d_fstage, sizeof(float) * 3 * N));
+  }
+  if (!c->first_step_done && !c->force_step_init) {
+    k_qm_to_pos<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_qm, c->d_pos, N);
+    c->force_step_init = true;
+  }
+  NNPE_CUDA(c, cudaMemcpyAsync(c->d_xstage, x_host, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, c->stream));
+  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_xstage, c->d_atom_id, c->d_xd, c->d_pos, N);
+  if (int rc = check_valid_enqueue(c)) return rc;
+  if (int rc = rebuild_enqueue(c, true)) return rc;
+  if (int rc = ghost_update_enqueue(c, true)) return rc;
+  const bool ev = erg || virial;
+  if (int rc = forces_enqueue(c, ev)) return rc;
+  if (ev) {
+    if (int rc = energy_reduce_enqueue(c, 0)) return rc;
+    NNPE_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+  }
+  k_gather_forces<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_frc, c->d_atom_id, c->d_fstage, N);
+  NNPE_CUDA(c, cudaMemcpyAsync(f_host, c->d_fstage, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (ev) {
+    if (erg) *erg = c->h_red[0];
+    if (virial) *virial = c->h_red[1];
+  }
+  return NNPE_OK;
+}
+
+extern "C" int nnpe_compute_forces(nnpe_ctx* c, int ev, double* erg, double* virial) {
+  if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_compute_forces: not set up");
+  cudaSetDevice(c->device);
+  if (int rc = forces_enqueue(c, ev != 0)) return rc;
+  if (ev) {
+    if (int rc = energy_reduce_enqueue(c, 0)) return rc;
+    NNPE_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (int rc = nnpe_sync_errors(c)) return rc;
+  if (ev) {
+    if (erg) *erg = c->h_red[0];
+    if (virial) *virial = c->h_red[1];
+  }
+  return NNPE_OK;
+}

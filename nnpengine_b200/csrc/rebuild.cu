@@ -1,0 +1,413 @@
+// List rebuild on the device: refold + cell binning, stable counting sort by cell, explicit
+// periodic images, image sort, molecule images for the bonded terms, and the full Verlet list.
+//
+// Every kernel takes the device rebuild flag and returns at once when it is clear, so that one
+// step is a fixed launch sequence (capturable in a CUDA graph) and the decision "is the list
+// still valid" (NEIGHLIST::isvalid, neighlist.cpp:178-187) never round-trips to the host.
+#include "internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ bool skip(const int* ctrl, bool cond) { return cond && ctrl[CTRL_REBUILD] == 0; }
+
+__global__ void k_zero_counts(int* a, int* b, int n, const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) { a[i] = 0; b[i] = 0; }
+}
+
+// LOCAL::refold_and_tag (environ.cpp:234-262): wrap x -= nearbyint(x*r_bl)*bl and bin.
+__global__ void k_refold_bin(double4* __restrict__ xd, int* __restrict__ ctmp, int* __restrict__ slot,
+                             int* __restrict__ ccount, int N, GridParams g, bool fp64, int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double4 x = xd[i];
+  float xf, yf, zf;
+  if (fp64) {
+    const double bl = (double)g.bl, rbl = 1.0 / bl;
+    x.x -= rint(x.x * rbl) * bl;
+    x.y -= rint(x.y * rbl) * bl;
+    x.z -= rint(x.z * rbl) * bl;
+    xf = (float)x.x; yf = (float)x.y; zf = (float)x.z;
+  } else {
+    xf = (float)x.x; yf = (float)x.y; zf = (float)x.z;
+    xf = fsub(xf, fmul(rintf(fmul(xf, g.r_bl)), g.bl));
+    yf = fsub(yf, fmul(rintf(fmul(yf, g.r_bl)), g.bl));
+    zf = fsub(zf, fmul(rintf(fmul(zf, g.r_bl)), g.bl));
+    x.x = xf; x.y = yf; x.z = zf;
+  }
+  xd[i] = x;
+  int c = cell_of(g, xf, yf, zf, ctrl + CTRL_ERR);
+  ctmp[i] = c;
+  slot[i] = atomicAdd(&ccount[c], 1);
+}
+
+// Exclusive scan of n counts by one block: start[k] = offset + sum(in[<k]), end[k] = start[k] + in[k].
+__global__ void k_scan(const int* __restrict__ in, int n, int* __restrict__ start, int* __restrict__ end, int offset,
+                       int* total, const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  __shared__ int warp_sums[32];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int chunk = (n + T - 1) / T;
+  const int k0 = min(n, t * chunk), k1 = min(n, k0 + chunk);
+  int local = 0;
+  for (int k = k0; k < k1; ++k) local += in[k];
+  // block exclusive scan of `local`
+  int v = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    int u = __shfl_up_sync(0xffffffffu, v, o);
+    if ((t & 31) >= o) v += u;
+  }
+  if ((t & 31) == 31) warp_sums[t >> 5] = v;
+  __syncthreads();
+  if (t < 32) {
+    int w = t < (T >> 5) ? warp_sums[t] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int u = __shfl_up_sync(0xffffffffu, w, o);
+      if (t >= o) w += u;
+    }
+    warp_sums[t] = w;
+  }
+  __syncthreads();
+  int prefix = v - local + ((t >> 5) ? warp_sums[(t >> 5) - 1] : 0) + offset;
+  for (int k = k0; k < k1; ++k) {
+    start[k] = prefix;
+    prefix += in[k];
+    if (end) end[k] = prefix;
+  }
+  if (t == T - 1 && total) *total = prefix;
+}
+
+__global__ void k_scatter(const int* __restrict__ ctmp, const int* __restrict__ slot, const int* __restrict__ cstart,
+                          int* __restrict__ perm, int N, int base, const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  perm[cstart[ctmp[i]] - base + slot[i]] = i;
+}
+
+__global__ void k_gscatter(const int* __restrict__ gcell, const int* __restrict__ gslot, const int* __restrict__ gcstart,
+                           int* __restrict__ perm, int Gcap, int base, const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  const int ng = min(ctrl[CTRL_NGHOST], Gcap);
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  perm[gcstart[gcell[g]] - base + gslot[g]] = g;
+}
+
+// Within each cell, order entries by their previous index: together with the counting sort this
+// is the stable sort of ENVIRON::sort / sort_ghost (environ.cpp:332-346, 384-389).
+constexpr int kSortWarps = 4, kSortCap = 1024;
+__global__ void __launch_bounds__(kSortWarps * 32) k_cell_sort(int* __restrict__ perm, const int* __restrict__ cstart,
+                                                               const int* __restrict__ cend, int ncell, int base,
+                                                               int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  __shared__ int buf[kSortWarps][kSortCap];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cidx = blockIdx.x * kSortWarps + w;
+  if (cidx >= ncell) return;
+  const int s = cstart[cidx] - base, n = cend[cidx] - cstart[cidx];
+  if (n <= 1) return;
+  if (n > kSortCap) {
+    if (lane == 0) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_CELL_OVERFLOW);
+    return;
+  }
+  int* b = buf[w];
+  for (int k = lane; k < n; k += 32) b[k] = perm[s + k];
+  __syncwarp();
+  for (int k = lane; k < n; k += 32) {
+    const int v = b[k];
+    int r = 0;
+    for (int m = 0; m < n; ++m) r += b[m] < v;
+    perm[s + r] = v;
+  }
+}
+
+// Gather the per-atom arrays into the new order (scratch), then copy back with derived fields.
+__global__ void k_gather(const int* __restrict__ perm, const double4* __restrict__ xd, const double4* __restrict__ vd,
+                         const float4* __restrict__ acc, const int2* __restrict__ info, const int* __restrict__ aid,
+                         const float2* __restrict__ qm, const int* __restrict__ ctmp, double4* __restrict__ sxd,
+                         double4* __restrict__ svd, float4* __restrict__ sacc, int2* __restrict__ sinfo,
+                         int* __restrict__ satom, float2* __restrict__ sqm, int* __restrict__ cell, int N,
+                         const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const int j = perm[k];
+  sxd[k] = xd[j]; svd[k] = vd[j]; sacc[k] = acc[j]; sinfo[k] = info[j]; satom[k] = aid[j]; sqm[k] = qm[j];
+  cell[k] = ctmp[j];
+}
+
+__global__ void k_copyback(const double4* __restrict__ sxd, const double4* __restrict__ svd, const float4* __restrict__ sacc,
+                           const int2* __restrict__ sinfo, const int* __restrict__ satom, const float2* __restrict__ sqm,
+                           double4* __restrict__ xd, double4* __restrict__ vd, float4* __restrict__ acc,
+                           int2* __restrict__ info, int* __restrict__ aid, float2* __restrict__ qm,
+                           float4* __restrict__ pos, int* __restrict__ sorted_of_id, int* __restrict__ molshift,
+                           int* __restrict__ gcnt, int N, GridParams g, const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const double4 x = sxd[k];
+  const int a = satom[k];
+  const float2 qq = sqm[k];
+  xd[k] = x; vd[k] = svd[k]; acc[k] = sacc[k]; info[k] = sinfo[k]; aid[k] = a; qm[k] = qq;
+  const float xf = (float)x.x, yf = (float)x.y, zf = (float)x.z;
+  pos[k] = make_float4(xf, yf, zf, qq.x);
+  sorted_of_id[a] = k;
+  molshift[a] = 13;
+  // number of periodic images of this atom (LOCAL::generate_ghost, environ.cpp:410-439)
+  const int xs = xf > g.ghost_lim ? -1 : 0, xe = xf < -g.ghost_lim ? 1 : 0;
+  const int ys = yf > g.ghost_lim ? -1 : 0, ye = yf < -g.ghost_lim ? 1 : 0;
+  const int zs = zf > g.ghost_lim ? -1 : 0, ze = zf < -g.ghost_lim ? 1 : 0;
+  int n = 0;
+  if (xs != xe || ys != ye || zs != ze) n = (xe - xs + 1) * (ye - ys + 1) * (ze - zs + 1) - 1;
+  gcnt[k] = n;
+}
+
+// Images in (owner, shift-loop) order, i.e. the order tidyup_ghost concatenates them
+// (environ.cpp:157-176 over threads owning ascending index ranges), with their cells.
+__global__ void k_ghost_emit(const float4* __restrict__ pos, const int* __restrict__ goff, int* __restrict__ gowner,
+                             int* __restrict__ gshift, int* __restrict__ gcell, int* __restrict__ gslot,
+                             int* __restrict__ gccount, int N, int Gcap, GridParams g, int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0 && ctrl[CTRL_NGHOST] > Gcap) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_GHOST_OVERFLOW);
+  if (k >= N) return;
+  const float4 p = pos[k];
+  const int xs = p.x > g.ghost_lim ? -1 : 0, xe = p.x < -g.ghost_lim ? 1 : 0;
+  const int ys = p.y > g.ghost_lim ? -1 : 0, ye = p.y < -g.ghost_lim ? 1 : 0;
+  const int zs = p.z > g.ghost_lim ? -1 : 0, ze = p.z < -g.ghost_lim ? 1 : 0;
+  if (xs == xe && ys == ye && zs == ze) return;
+  int o = goff[k];
+  for (int ix = xs; ix <= xe; ++ix)
+    for (int iy = ys; iy <= ye; ++iy)
+      for (int iz = zs; iz <= ze; ++iz) {
+        if (!ix && !iy && !iz) continue;
+        const int gg = o++;
+        if (gg >= Gcap) continue;
+        const int code = (ix + 1) * 9 + (iy + 1) * 3 + (iz + 1);
+        float s[3];
+        shift_of(g, code, s);
+        // ghost position x_owner + shift (environ.cpp:505-507)
+        const int c = cell_of(g, fadd(p.x, s[0]), fadd(p.y, s[1]), fadd(p.z, s[2]), ctrl + CTRL_ERR);
+        gowner[gg] = k;
+        gshift[gg] = code;
+        gcell[gg] = c;
+        gslot[gg] = atomicAdd(&gccount[c], 1);
+      }
+}
+
+// Sorted images: position, info, owner; molecule images for the bonded terms
+// (update_ghost_and_info, environ.cpp:444-470).
+__global__ void k_ghost_gather(const int* __restrict__ perm, const int* __restrict__ tgowner, const int* __restrict__ tgshift,
+                               const int* __restrict__ tgcell, int* __restrict__ gowner, int* __restrict__ gshift,
+                               float4* __restrict__ pos, int2* __restrict__ info, int* __restrict__ cell,
+                               const int* __restrict__ aid, const int* __restrict__ sorted_of_id,
+                               const int* __restrict__ mol_rep, int* __restrict__ molshift, int N, int Gcap,
+                               GridParams g, const int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  const int ng = min(ctrl[CTRL_NGHOST], Gcap);
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ng) return;
+  const int src = perm[k];
+  const int owner = tgowner[src], code = tgshift[src];
+  gowner[k] = owner;
+  gshift[k] = code;
+  float s[3];
+  shift_of(g, code, s);
+  const float4 p = pos[owner];
+  const float4 q = make_float4(fadd(p.x, s[0]), fadd(p.y, s[1]), fadd(p.z, s[2]), p.w);
+  pos[N + k] = q;
+  const int2 inf = info[owner];
+  info[N + k] = inf;
+  cell[N + k] = tgcell[src];
+  if (info_intra(inf) != 0) {
+    const int rep = sorted_of_id[mol_rep[inf.x]];
+    const float4 r = pos[rep];
+    if (fabsf(fsub(q.x, r.x)) < g.h_bl && fabsf(fsub(q.y, r.y)) < g.h_bl && fabsf(fsub(q.z, r.z)) < g.h_bl)
+      molshift[aid[owner]] = code;
+  }
+}
+
+// NEIGHLIST::build<true> (neighlist.cpp:190-331): one warp per atom walks the stencil rows of
+// its cell, real atoms first then images, and appends accepted candidates in index order.
+// A candidate is accepted without a distance test when its cell carries the no-check bit
+// (NEGH_USE_INNERCUT), else when rsq < (cutoff+skin)^2 in the reference's float sequence.
+__global__ void __launch_bounds__(128) k_build_list(const float4* __restrict__ pos, const int2* __restrict__ info,
+                                                    const int* __restrict__ cell, const int* __restrict__ cstart,
+                                                    const int* __restrict__ cend, const int* __restrict__ gcstart,
+                                                    const int* __restrict__ gcend, const int4* __restrict__ rows,
+                                                    const int* __restrict__ nrows, int maxrows,
+                                                    const int* __restrict__ special, int nmax,
+                                                    uint32_t* __restrict__ list, int* __restrict__ ncount,
+                                                    float4* __restrict__ xbuild, int N, int cap, float cutsq,
+                                                    int* ctrl, bool cond) {
+  if (skip(ctrl, cond)) return;
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= N) return;
+  const float4 xi = pos[i];
+  const int2 infi = info[i];
+  const int ci = cell[i];
+  const int* spi = special + (info_moltype(infi) * nmax + info_intra(infi)) * nmax;
+  uint32_t* row_out = list + (size_t)i * cap;
+  const int nr = nrows[ci];
+  const int4* R = rows + (size_t)ci * maxrows;
+  int cnt = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int r = 0; r < nr; ++r) {
+      const int4 row = R[r];
+      const int j0 = pass ? gcstart[row.x] : cstart[row.x];
+      const int j1 = pass ? gcend[row.y] : cend[row.y];
+      for (int base = j0; base < j1; base += 32) {
+        const int j = base + lane;
+        bool ok = false;
+        if (j < j1 && (pass || j != i)) {
+          const int cj = cell[j];
+          if ((row.z >> (cj - row.x)) & 1) ok = true;
+          else {
+            const float4 xj = pos[j];
+            ok = rsq3(fsub(xi.x, xj.x), fsub(xi.y, xj.y), fsub(xi.z, xj.z)) < cutsq;
+          }
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+          const int2 infj = info[j];
+          const int s = infj.x == infi.x ? spi[info_intra(infj)] : 0;
+          const int idx = cnt + __popc(b & ((1u << lane) - 1));
+          if (idx < cap) row_out[idx] = (uint32_t)j | ((uint32_t)info_type(infj) << 27) | ((uint32_t)s << 30);
+        }
+        cnt += __popc(b);
+      }
+    }
+  }
+  if (lane == 0) {
+    ncount[i] = min(cnt, cap);
+    xbuild[i] = xi;
+    if (cnt >= cap) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_LIST_OVERFLOW);
+  }
+}
+
+// update_ghost_pos<false> (environ.cpp:515-520) every step; after a rebuild it recomputes the
+// same values. Thread 0 also retires the rebuild flag and counts the build (NEIGHLIST::nbuild).
+__global__ void k_ghost_update(float4* __restrict__ pos, const int* __restrict__ gowner, const int* __restrict__ gshift,
+                               int N, int Gcap, GridParams g, int* ctrl) {
+  const int ng = min(ctrl[CTRL_NGHOST], Gcap);
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < ng) {
+    float s[3];
+    shift_of(g, gshift[k], s);
+    const float4 p = pos[gowner[k]];
+    pos[N + k] = make_float4(fadd(p.x, s[0]), fadd(p.y, s[1]), fadd(p.z, s[2]), p.w);
+  }
+}
+
+__global__ void k_finish_rebuild(int* ctrl) {
+  if (ctrl[CTRL_REBUILD]) {
+    ctrl[CTRL_REBUILD] = 0;
+    ctrl[CTRL_NBUILD] += 1;
+  }
+}
+
+// isvalid: any atom displaced more than skin/2 since the last build (neighlist.cpp:178-187).
+__global__ void k_check_valid(const float4* __restrict__ pos, const float4* __restrict__ xbuild, int N, float dx2,
+                              int* ctrl) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float4 a = pos[i], b = xbuild[i];
+  if (rsq3(fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)) > dx2) ctrl[CTRL_REBUILD] = 1;
+}
+
+}  // namespace
+
+int rebuild_enqueue(nnpe_ctx* c, bool cond) {
+  const int N = c->natom, G = c->Gcap, NG = c->grid.num_grid;
+  cudaStream_t st = c->stream;
+  const GridParams g = c->grid;
+  int* ctrl = c->d_ctrl;
+  const int T = 256;
+  k_zero_counts<<<nblocks(NG, T), T, 0, st>>>(c->d_ccount, c->d_gccount, NG, ctrl, cond);
+  k_refold_bin<<<nblocks(N, T), T, 0, st>>>(c->d_xd, c->d_ctmp, c->d_slot, c->d_ccount, N, g, c->fp64_state, ctrl, cond);
+  k_scan<<<1, 1024, 0, st>>>(c->d_ccount, NG, c->d_cstart, c->d_cend, 0, nullptr, ctrl, cond);
+  k_scatter<<<nblocks(N, T), T, 0, st>>>(c->d_ctmp, c->d_slot, c->d_cstart, c->d_perm, N, 0, ctrl, cond);
+  k_cell_sort<<<nblocks(NG, kSortWarps), kSortWarps * 32, 0, st>>>(c->d_perm, c->d_cstart, c->d_cend, NG, 0, ctrl, cond);
+  k_gather<<<nblocks(N, T), T, 0, st>>>(c->d_perm, c->d_xd, c->d_vd, c->d_acc, c->d_info, c->d_atom_id, c->d_qm, c->d_ctmp,
+                                        c->d_sxd, c->d_svd, c->d_sacc, c->d_sinfo, c->d_satom, c->d_sqm, c->d_cell, N, ctrl, cond);
+  k_copyback<<<nblocks(N, T), T, 0, st>>>(c->d_sxd, c->d_svd, c->d_sacc, c->d_sinfo, c->d_satom, c->d_sqm, c->d_xd, c->d_vd,
+                                          c->d_acc, c->d_info, c->d_atom_id, c->d_qm, c->d_pos, c->d_sorted_of_id,
+                                          c->d_molshift, c->d_gcnt, N, g, ctrl, cond);
+  k_scan<<<1, 1024, 0, st>>>(c->d_gcnt, N, c->d_goff, nullptr, 0, ctrl + CTRL_NGHOST, ctrl, cond);
+  k_ghost_emit<<<nblocks(N, T), T, 0, st>>>(c->d_pos, c->d_goff, c->d_gtmp_owner, c->d_gtmp_shift, c->d_gtmp_cell,
+                                            c->d_gtmp_slot, c->d_gccount, N, G, g, ctrl, cond);
+  k_scan<<<1, 1024, 0, st>>>(c->d_gccount, NG, c->d_gcstart, c->d_gcend, N, nullptr, ctrl, cond);
+  k_gscatter<<<nblocks(G, T), T, 0, st>>>(c->d_gtmp_cell, c->d_gtmp_slot, c->d_gcstart, c->d_perm, G, N, ctrl, cond);
+  k_cell_sort<<<nblocks(NG, kSortWarps), kSortWarps * 32, 0, st>>>(c->d_perm, c->d_gcstart, c->d_gcend, NG, N, ctrl, cond);
+  k_ghost_gather<<<nblocks(G, T), T, 0, st>>>(c->d_perm, c->d_gtmp_owner, c->d_gtmp_shift, c->d_gtmp_cell, c->d_gowner,
+                                              c->d_gshift, c->d_pos, c->d_info, c->d_cell, c->d_atom_id, c->d_sorted_of_id,
+                                              c->d_mol_rep, c->d_molshift, N, G, g, ctrl, cond);
+  const float cs = c->pair_cutoff + c->skin;
+  k_build_list<<<nblocks((long)N * 32, 128), 128, 0, st>>>(
+      c->d_pos, c->d_info, c->d_cell, c->d_cstart, c->d_cend, c->d_gcstart, c->d_gcend, c->st_pair.rows, c->st_pair.nrows,
+      c->st_pair.maxrows, c->d_special, c->nmax, c->d_list, c->d_ncount, c->d_xbuild, N, c->cap, cs * cs, ctrl, cond);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int ghost_update_enqueue(nnpe_ctx* c, bool) {
+  k_ghost_update<<<nblocks(c->Gcap, 256), 256, 0, c->stream>>>(c->d_pos, c->d_gowner, c->d_gshift, c->natom, c->Gcap,
+                                                               c->grid, c->d_ctrl);
+  k_finish_rebuild<<<1, 1, 0, c->stream>>>(c->d_ctrl);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int check_valid_enqueue(nnpe_ctx* c) {
+  const float h = c->skin / 2;
+  k_check_valid<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_pos, c->d_xbuild, c->natom, h * h, c->d_ctrl);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+static int sync_errors(nnpe_ctx* c) {
+  NNPE_CUDA(c, cudaMemcpyAsync(c->h_ctrl, c->d_ctrl, sizeof(int) * CTRL_WORDS, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int e = c->h_ctrl[CTRL_ERR];
+  if (e & NNPE_DEV_LIST_OVERFLOW) return nnpe_fail(c, NNPE_EOVERFLOW, "nei_list overflow");
+  if (e & NNPE_DEV_GHOST_OVERFLOW) return nnpe_fail(c, NNPE_EOVERFLOW, "ghost overflow");
+  if (e & NNPE_DEV_CELL_OVERFLOW) return nnpe_fail(c, NNPE_EOVERFLOW, "cell overflow in sort");
+  if (e & NNPE_DEV_CELL_RANGE) return nnpe_fail(c, NNPE_ERANGE, "atom outside the cell grid");
+  return 0;
+}
+
+int nnpe_sync_errors(nnpe_ctx* c) { return sync_errors(c); }
+
+extern "C" int nnpe_list_build(nnpe_ctx* c) {
+  if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_list_build: not set up");
+  cudaSetDevice(c->device);
+  int one = 1;
+  NNPE_CUDA(c, cudaMemcpyAsync(c->d_ctrl + CTRL_REBUILD, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (int rc = rebuild_enqueue(c, true)) return rc;
+  if (int rc = ghost_update_enqueue(c, true)) return rc;
+  return sync_errors(c);
+}
+
+extern "C" int nnpe_list_isvalid(nnpe_ctx* c, int* valid) {
+  if (!c || !c->have_setup || !valid) return nnpe_fail(c, NNPE_EARG, "nnpe_list_isvalid");
+  cudaSetDevice(c->device);
+  NNPE_CUDA(c, cudaMemcpyAsync(c->h_ctrl, c->d_ctrl, sizeof(int) * CTRL_WORDS, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (c->h_ctrl[CTRL_REBUILD]) { *valid = 0; return NNPE_OK; }
+  if (int rc = check_valid_enqueue(c)) return rc;
+  NNPE_CUDA(c, cudaMemcpyAsync(c->h_ctrl, c->d_ctrl, sizeof(int) * CTRL_WORDS, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  *valid = c->h_ctrl[CTRL_REBUILD] ? 0 : 1;
+  return NNPE_OK;
+}
+
+extern "C" int nnpe_ghost_update(nnpe_ctx* c) {
+  if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_ghost_update");
+  k_ghost_update<<<nblocks(c->Gcap, 256), 256, 0, c->stream>>>(c->d_pos, c->d_gowner, c->d_gshift, c->natom, c->Gcap,
+                                                               c->grid, c->d_ctrl);
+  NNPE_CHECK_LAUNCH(c);
+  return NNPE_OK;
+}

@@ -1,0 +1,74 @@
+"""Seeded parity cases shared by the golden-fixture generator and the tests.
+
+Each case is a small system in the reference's own formats, with the water model of the
+3000-atom / 96k-atom workloads (O-H bond 1.0 A with k=450 kcal/mol/A^2, H-O-H 109.47 deg
+harmonic in cos(theta) with kc=62 kcal/mol, tabulated O-O LJ at 10 A with 1000 bins, DSF
+Coulomb, 2 A skin) or the two-species LJ+Coulomb mixture of the g(r)/S(q) workload.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+from typing import Dict
+
+import numpy as np
+
+from nnpengine_b200 import systems as S
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+WATER_BOND_K = 450.0
+WATER_ANGLE_KC = 62.0
+
+
+def water_case(n_side=6, bl=18.624, seed=1, temperature=300.0, nmol=None):
+    s = S.water_box(n_side, bl, seed=seed, temperature=temperature, nmol=nmol)
+    r, F, U = S.water_lj_table(10.0, 1000)
+    return s, (r, F, U)
+
+
+def mixture_case(natom=2000, rho=0.035, seed=4):
+    s = S.lj_mixture(natom, rho, 0.6, seed=seed)
+    r, F, U = S.lj_table(2, (3.0, 3.4), (0.15, 0.25), 10.0, 1000)
+    return s, (r, F, U)
+
+
+def table_as_loaded(F, U):
+    """The tables as the reference holds them after reading the %.9e text: float32, extra zero column."""
+    F = np.asarray(F, np.float64).astype(np.float32)
+    U = np.asarray(U, np.float64).astype(np.float32)
+    z = np.zeros((F.shape[0], 1), np.float32)
+    return np.concatenate([F, z], 1), np.concatenate([U, z], 1)
+
+
+def write_inputs(s, table, d) -> Dict[str, str]:
+    """Write the reference-format inputs of a case into directory d."""
+    os.makedirs(d, exist_ok=True)
+    init = os.path.join(d, "init.txt")
+    S.write_init_file(init, s)
+    tab = os.path.join(d, "table.txt")
+    r, F, U = table
+    S.write_pair_table(tab, r, F, U)
+    vel = os.path.join(d, "v.bin")
+    S.write_velocity_file(vel, s.v)
+    return dict(init=init, table=tab, vel=vel)
+
+
+def list_keys(rec: np.ndarray, natom: int):
+    """Per-atom sorted neighbour keys (id_j, image, special) and a digest per atom."""
+    rec = np.asarray(rec, np.int64)
+    key = (rec[:, 1] * 27 + rec[:, 2]) * 4 + rec[:, 3]
+    order = np.lexsort((key, rec[:, 0]))
+    i_sorted, k_sorted = rec[order, 0], key[order]
+    counts = np.bincount(i_sorted, minlength=natom)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    digests = np.zeros(natom, np.uint64)
+    for a in range(natom):
+        h = hashlib.blake2b(k_sorted[starts[a]:starts[a + 1]].tobytes(), digest_size=8).digest()
+        digests[a] = np.frombuffer(h, np.uint64)[0]
+    return counts, digests
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))

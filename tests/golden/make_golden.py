@@ -1,0 +1,76 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference's own C++.
+
+The reference (NNPEngine src/, compiled in place by oracle/Makefile into oracle/_ref/ref_dump)
+is run on the seeded cases of tests/cases.py; its outputs are stored compactly:
+
+* water648.npz   648-atom water box (6^3 molecules, 18.624 A): per-atom full-list counts and
+                 digests of the sorted (id_j, image, special) keys; forces and energy/virial of one
+                 force evaluation (pair + bond + angle); cell-based and list-based g(r) counts; a
+                 20-step NVE trajectory in the reference's float arithmetic (final x, v and the
+                 per-step energies).
+* mixture2000.npz  2000-atom two-species LJ+Coulomb liquid at 0.035 A^-3: g(r) counts to 15 A in
+                 0.01 A bins, the reference's float g(r) and S(q) on 512 q points, forces.
+
+Run:  python tests/golden/make_golden.py   (needs /root/reference/src and `make -C oracle ref`).
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from oracle import orc  # noqa: E402
+import cases  # noqa: E402
+
+
+def bonded_cfg():
+    return {"bond": [f"1.0 {cases.WATER_BOND_K}"], "angle": [f"109.47 0 0 {cases.WATER_ANGLE_KC}"]}
+
+
+def water648(work):
+    s, table = cases.water_case()
+    f = cases.write_inputs(s, table, work)
+    v0 = os.path.join(work, "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    base = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10, **bonded_cfg()}
+    snap = orc.run_ref_dump({**base, "velocity": v0, "mode": "snapshot"}, os.path.join(work, "snap"))
+    counts, digests = cases.list_keys(snap["fulllist"], s.natom)
+    md = orc.run_ref_dump({**base, "velocity": f["vel"], "mode": "md", "steps": 20, "dt": 1, "log_interval": 1},
+                          os.path.join(work, "md"))
+    out = dict(x=s.x, v=s.v, list_counts=counts, list_digests=digests, nghost=snap["info"]["nghost"],
+               force=snap["force"].reshape(-1, 3), erg_f32=snap["log_e"], vir_f32=snap["log_w"],
+               gr_counts=snap["gr_counts"].reshape(3, -1), gr_inner_counts=snap["gr_inner_counts"].reshape(3, -1),
+               md_x=md["x"].reshape(-1, 3), md_v=md["v"].reshape(-1, 3), md_erg=md["log_e"], md_ekin=md["log_k"],
+               md_nbuild=md["info"]["nbuild_last"])
+    np.savez_compressed(os.path.join(HERE, "water648.npz"), **out)
+    print("water648:", s.natom, "atoms,", int(counts.sum()), "list entries,", snap["info"]["nghost"], "images")
+
+
+def mixture2000(work):
+    s, table = cases.mixture_case()
+    f = cases.write_inputs(s, table, work)
+    v0 = os.path.join(work, "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    snap = orc.run_ref_dump({"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2,
+                             "gr_cutoff": 15, "nq": 512, "qmax": 20, "velocity": v0, "mode": "snapshot"},
+                            os.path.join(work, "snap"))
+    counts, digests = cases.list_keys(snap["fulllist"], s.natom)
+    out = dict(x=s.x, v=s.v, typ=s.typ, list_counts=counts, list_digests=digests,
+               force=snap["force"].reshape(-1, 3), erg_f32=snap["log_e"],
+               gr_counts=snap["gr_counts"].reshape(3, -1), gr_inner_counts=snap["gr_inner_counts"].reshape(3, -1),
+               gr_f32=snap["gr"].reshape(3, -1), sq_f32=snap["sq"].reshape(3, -1), qq=snap["qq"])
+    np.savez_compressed(os.path.join(HERE, "mixture2000.npz"), **out)
+    print("mixture2000:", s.natom, "atoms, gr bins", out["gr_counts"].shape)
+
+
+if __name__ == "__main__":
+    with tempfile.TemporaryDirectory() as t:
+        water648(os.path.join(t, "w"))
+        mixture2000(os.path.join(t, "m"))

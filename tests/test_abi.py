@@ -1,0 +1,47 @@
+"""The C-ABI library: it loads, exports every declared symbol, and fails cleanly without a GPU."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from nnpengine_b200 import _lib, systems
+
+
+def test_library_exports_declared_symbols():
+    lib = _lib.load()
+    declared = _lib.declared_symbols()
+    assert len(declared) > 30
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_coef_helpers_match_reference_set_param():
+    from nnpengine_b200 import engine
+    np.testing.assert_array_equal(engine.bond_coef(1.0, 0, 0, 450.0), np.array([1, 0, 0, 900], np.float32))
+    a = engine.angle_coef(109.47, 0, 0, 62.0)
+    assert a[0] == np.float32(np.cos(np.float32(109.47) * np.float32(np.pi) / np.float32(180)))
+    np.testing.assert_array_equal(engine.dihedral_coef(1, 2, 3, 4), np.array([1 - 3, 2 - 12, 12, 48], np.float32))
+
+
+def test_create_without_device_reports_error():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = _lib.load()
+    h = C.c_void_p()
+    assert lib.nnpe_create(0, C.byref(h)) != 0
+
+
+def test_water_files_roundtrip(tmp_path):
+    s = systems.water_box(3, 9.312, seed=3)
+    p = tmp_path / "init.txt"
+    systems.write_init_file(str(p), s)
+    lines = [l for l in open(p).read().splitlines() if l.strip()]
+    nmt, nmol = map(int, lines[0].split())
+    assert (nmt, nmol) == (1, 27)
+    ntype, natom, bl = lines[2].split()
+    assert int(natom) == 81 and abs(float(bl) - 9.312) < 1e-6
+    x = np.array([[float(v) for v in l.split()[4:7]] for l in lines[3:]], np.float32)
+    np.testing.assert_array_equal(x, s.x)
+    mol = open(str(p).replace("init.txt", "init.mol0")).read()
+    assert "3 atoms" in mol and "Bonds" in mol and "Angles" in mol

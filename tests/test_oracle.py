@@ -1,0 +1,98 @@
+"""The oracle (C restatement) against the golden vectors produced by the reference's own C++."""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from oracle import orc
+
+pytestmark = pytest.mark.skipif(not os.path.exists(os.path.join(orc.BUILD_DIR, "liboracle_f32.so")),
+                                reason="oracle not built")
+
+
+def _water():
+    g = np.load(os.path.join(cases.GOLDEN, "water648.npz"))
+    s, table = cases.water_case()
+    np.testing.assert_array_equal(s.x, g["x"])      # the seeded generator is reproducible
+    return s, table, g
+
+
+def _bonded():
+    from nnpengine_b200.systems import WATER
+    return (np.array([[1.0, 0, 0, 2 * cases.WATER_BOND_K]], np.float32),
+            np.array([[np.cos(np.float32(109.47) * np.float32(np.pi) / np.float32(180)), 0, 0,
+                       2 * cases.WATER_ANGLE_KC]], np.float32),
+            np.zeros((1, 4), np.float32))
+
+
+def test_restated_list_matches_reference_bit_exact():
+    s, table, g = _water()
+    o = orc.Restated(s, "f32")
+    assert o.rebuild(s.x, 10, 2, 12) == 0
+    assert o.nghost == int(g["nghost"])
+    counts, digests = cases.list_keys(o.list_records(), s.natom)
+    np.testing.assert_array_equal(counts, g["list_counts"])
+    np.testing.assert_array_equal(digests, g["list_digests"])
+
+
+def test_restated_forces_match_reference():
+    s, table, g = _water()
+    F, U = cases.table_as_loaded(table[1], table[2])
+    o = orc.Restated(s, "f32")
+    o.rebuild(s.x, 10, 2, 12)
+    f, e, w = o.pair_forces(F, U, 10.0)
+    fb, eb, wb = o.bonded(*_bonded())
+    assert cases.rel_rms(f + fb, g["force"]) < 1e-5
+    # the reference accumulates its energy in float; the restatement sums the same terms in double
+    assert abs((e + eb) - g["erg_f32"][0]) / abs(g["erg_f32"][0]) < 1e-4
+    assert abs((w + wb) - g["vir_f32"][0]) / abs(g["vir_f32"][0]) < 1e-4
+
+
+def test_fp64_oracle_close_to_fp32():
+    s, table, g = _water()
+    F, U = cases.table_as_loaded(table[1], table[2])
+    o = orc.Restated(s, "f64")
+    o.rebuild(s.x, 10, 2, 12)
+    f, e, w = o.pair_forces(F, U, 10.0)
+    fb, eb, wb = o.bonded(*_bonded())
+    assert cases.rel_rms(f + fb, g["force"]) < 1e-5
+
+
+def test_restated_gr_counts_bit_exact():
+    s, table, g = _water()
+    o = orc.Restated(s, "f32")
+    o.rebuild(s.x, 10, 2, 12)
+    np.testing.assert_array_equal(o.gr_counts(10, 2, 1000, 10), g["gr_counts"])
+
+
+def test_restated_mixture_gr_and_sq():
+    gm = np.load(os.path.join(cases.GOLDEN, "mixture2000.npz"))
+    s, table = cases.mixture_case()
+    np.testing.assert_array_equal(s.x, gm["x"])
+    o = orc.Restated(s, "f32")
+    assert o.rebuild(s.x, 10, 2, 17) == 0
+    counts, digests = cases.list_keys(o.list_records(), s.natom)
+    np.testing.assert_array_equal(counts, gm["list_counts"])
+    np.testing.assert_array_equal(digests, gm["list_digests"])
+    cnt = o.gr_counts(15, 2, 1000, 10)
+    np.testing.assert_array_equal(cnt, gm["gr_counts"])
+    # S(q) of the reference's float g(r): FP64 transform agrees with its float transform
+    sq, qq = orc.sq(s.natom, s.bl, gm["gr_f32"].astype(np.float64), np.float32(10) / np.float32(1000), 512, 20.0)
+    np.testing.assert_allclose(qq, gm["qq"], rtol=1e-6)
+    scale = np.abs(gm["sq_f32"]).max()
+    assert np.abs(sq - gm["sq_f32"]).max() < 1e-3 * scale
+
+
+@pytest.mark.skipif(not orc.ref_available(), reason="reference harness not built")
+def test_reference_harness_reproducible(tmp_path):
+    """Re-running the reference gives the committed fixture (seeded inputs, deterministic sums)."""
+    s, table, g = _water()
+    f = cases.write_inputs(s, table, str(tmp_path))
+    v0 = str(tmp_path / "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    r = orc.run_ref_dump({"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10,
+                          "bond": [f"1.0 {cases.WATER_BOND_K}"], "angle": [f"109.47 0 0 {cases.WATER_ANGLE_KC}"],
+                          "velocity": v0, "mode": "snapshot"}, str(tmp_path / "o"))
+    np.testing.assert_array_equal(r["force"].reshape(-1, 3), g["force"])
+    np.testing.assert_array_equal(r["gr_counts"].reshape(3, -1), g["gr_counts"])
