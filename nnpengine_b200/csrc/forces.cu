@@ -14,6 +14,9 @@ constexpr float kElectricK = 332.06371f;
 
 struct PairParams {
   const float4* pos;
+  const int* gowner;
+  const int* gshift;
+  GridParams g;
   const uint32_t* list;
   const int* ncount;
   const int2* info;
@@ -30,6 +33,40 @@ struct PairParams {
 // One warp per atom: lanes stride over the atom's list row (coalesced 128-byte reads), gather
 // neighbour positions, and reduce with shuffles; the warp writes the atom's force once (no
 // atomics, deterministic).
+// Exact double coordinates of list entry j: a real atom's float position, or its owner's float
+// position plus the float box shift added in double (the image the float list entry rounds).
+__device__ __forceinline__ double3 exact_pos(const PairParams& p, int j) {
+  if (j < p.N) {
+    const float4 x = p.pos[j];
+    return make_double3(x.x, x.y, x.z);
+  }
+  const int k = j - p.N;
+  const float4 x = p.pos[p.gowner[k]];
+  float s[3];
+  shift_of(p.g, p.gshift[k], s);
+  return make_double3((double)x.x + (double)s[0], (double)x.y + (double)s[1], (double)x.z + (double)s[2]);
+}
+
+// FP64 pair energy and fpair*rsq of one pair at double separation: the energy/virial reductions of
+// ev steps (pair.cpp:365-410) evaluated in double so that cancellation in the Coulomb sum does not
+// leave FP32 rounding in the total.
+__device__ __forceinline__ void pair_energy64(const PairParams& p, const float2* tab0, int s, double qq, double rsq,
+                                              double* e, double* w) {
+  const double rc = p.cutoff;
+  if (!(rsq < rc * rc)) return;
+  const double r = sqrt(rsq);
+  double u = r * (double)p.r_dr - 0.5;
+  const int t1 = (int)u;
+  const double w2 = u - t1, w1 = 1 - w2;
+  const float2 a = tab0[t1], b = tab0[t1 + 1];
+  const double slj = c_special_lj[s], sco = s == 3 ? 5.0 / 6.0 : (double)c_special_coul[s];
+  const double vc = -1 / rc, fc = vc / rc;
+  const double fpair = ((double)a.x * w1 + (double)b.x * w2) * slj + qq * (1 / (r * rsq) + fc / r) * sco;
+  const double ue = ((double)a.y * w1 + (double)b.y * w2) * slj + qq * (1 / r + vc + fc * (rc - r)) * sco;
+  *e += 0.5 * ue;
+  *w += 0.5 * fpair * rsq;
+}
+
 template <bool EV>
 __global__ void __launch_bounds__(128) k_pair(PairParams p) {
   const int lane = threadIdx.x & 31;
@@ -61,12 +98,13 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
       const float qq = xi.w * xj.w * kElectricK;
       fpair += qq * (1 / (r * rsq) + p.fc / r) * c_special_coul[s];
       fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
-      if (EV) {
-        const float u = (a.y * ipw1 + b.y * ipw2) * c_special_lj[s] +
-                        qq * (1 / r + p.vc + p.fc * (p.cutoff - r)) * c_special_coul[s];
-        e += 0.5 * (double)u;
-        w += 0.5 * (double)(fpair * rsq);
-      }
+    }
+    if (EV) {
+      const double3 xjd = exact_pos(p, j);
+      const double ddx = (double)xi.x - xjd.x, ddy = (double)xi.y - xjd.y, ddz = (double)xi.z - xjd.z;
+      const int tj = (ent >> 27) & 7, s = ent >> 30;
+      pair_energy64(p, p.table + (size_t)ptrow[tj] * (p.nbin + 1), s, (double)xi.w * (double)xj.w * 332.06371,
+                    ddx * ddx + ddy * ddy + ddz * ddz, &e, &w);
     }
   }
 #pragma unroll
@@ -134,13 +172,20 @@ __device__ __forceinline__ void addf(float4* frc, int s, float fx, float fy, flo
   frc[s] = make_float4(f.x + fx, f.y + fy, f.z + fz, f.w);
 }
 
+__device__ __forceinline__ double3 xmol64(const BondedParams& p, int a) {
+  const float4 x = p.pos[p.sorted_of_id[a]];
+  float sh[3];
+  shift_of(p.g, p.molshift[a], sh);
+  return make_double3((double)x.x + sh[0], (double)x.y + sh[1], (double)x.z + sh[2]);
+}
+
 // One thread per molecule evaluates all of its bonded terms (molecules never share atoms, so
 // the read-modify-write of the atoms' forces is race free).
 template <bool EV>
 __global__ void k_bonded(BondedParams p) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= p.nmol) return;
-  float e = 0.f, w = 0.f;
+  double e = 0.0, w = 0.0;
   const int b0 = p.terms[3 * m], b1 = p.terms[3 * m + 3];
   for (int t = b0; t < b1; ++t) {
     const int4 b = p.bond[t];
@@ -155,17 +200,21 @@ __global__ void k_bonded(BondedParams p) {
     dx *= ff; dy *= ff; dz *= ff;
     addf(p.frc, si, -dx, -dy, -dz);
     addf(p.frc, sj, dx, dy, dz);
-    if (EV) {
-      e += 0.5F * (dr * dr) * (c.y * (bdr * bdr) + c.w);
-      w -= ff * rr * rr;
+    if (EV) {   // bond.cpp:131-135 in FP64
+      const double3 a = xmol64(p, b.y), bb = xmol64(p, b.z);
+      const double ex = a.x - bb.x, ey = a.y - bb.y, ez = a.z - bb.z;
+      const double r = sqrt(ex * ex + ey * ey + ez * ez);
+      const double d = r - c.x, bd = c.z - d;
+      e += 0.5 * d * d * (c.y * bd * bd + c.w);
+      w -= d * (c.w + c.y * bd * (bd - d)) / r * r * r;
     }
   }
   const int a0 = p.terms[3 * m + 1], a1 = p.terms[3 * m + 4];
   for (int t = a0; t < a1; ++t) {
-    const int4 a = p.angle[t];
-    const float4 c = p.acoef[a.x];
+    const int4 a4 = p.angle[t];
+    const float4 c = p.acoef[a4.x];
     int si, sj, sk;
-    const float3 xi = xmol(p, a.y, &si), xj = xmol(p, a.z, &sj), xk = xmol(p, a.w, &sk);
+    const float3 xi = xmol(p, a4.y, &si), xj = xmol(p, a4.z, &sj), xk = xmol(p, a4.w, &sk);
     float dx1 = xi.x - xj.x, dy1 = xi.y - xj.y, dz1 = xi.z - xj.z;
     float dx2 = xk.x - xj.x, dy2 = xk.y - xj.y, dz2 = xk.z - xj.z;
     const float r_r1 = 1 / sqrtf(dx1 * dx1 + dy1 * dy1 + dz1 * dz1);
@@ -184,7 +233,14 @@ __global__ void k_bonded(BondedParams p) {
     fx = ff * (dx1 - cq * dx2); fy = ff * (dy1 - cq * dy2); fz = ff * (dz1 - cq * dz2);
     addf(p.frc, sk, -fx, -fy, -fz);
     addf(p.frc, sj, fx, fy, fz);
-    if (EV) e += 0.5F * (dcq * dcq) * (c.y * (b_dcq * b_dcq) + c.w);
+    if (EV) {   // angle.cpp:289-292 in FP64
+      const double3 a = xmol64(p, a4.y), bb = xmol64(p, a4.z), cc = xmol64(p, a4.w);
+      const double u1x = a.x - bb.x, u1y = a.y - bb.y, u1z = a.z - bb.z, u2x = cc.x - bb.x, u2y = cc.y - bb.y, u2z = cc.z - bb.z;
+      const double cqd = (u1x * u2x + u1y * u2y + u1z * u2z) /
+                         sqrt((u1x * u1x + u1y * u1y + u1z * u1z) * (u2x * u2x + u2y * u2y + u2z * u2z));
+      const double d = cqd - c.x, bd = c.z - d;
+      e += 0.5 * d * d * (c.y * bd * bd + c.w);
+    }
   }
   const int d0 = p.terms[3 * m + 2], d1 = p.terms[3 * m + 5];
   for (int t = d0; t < d1; ++t) {
@@ -214,7 +270,19 @@ __global__ void k_bonded(BondedParams p) {
     addf(p.frc, sl, f3x, f3y, f3z);
     addf(p.frc, sj, f2x - f1x, f2y - f1y, f2z - f1z);
     addf(p.frc, sk, -(f2x + f3x), -(f2y + f3y), -(f2z + f3z));
-    if (EV) e += ((c.w / 3 * cq + c.z / 2) * cq + c.y) * cq + c.x;
+    if (EV) {   // dihedral.cpp:454-458 in FP64
+      const double3 a = xmol64(p, d[1]), bb = xmol64(p, d[2]), cc = xmol64(p, d[3]), dd = xmol64(p, d[4]);
+      double v1x = a.x - bb.x, v1y = a.y - bb.y, v1z = a.z - bb.z;
+      const double v2x = cc.x - bb.x, v2y = cc.y - bb.y, v2z = cc.z - bb.z;
+      double v3x = dd.x - cc.x, v3y = dd.y - cc.y, v3z = dd.z - cc.z;
+      const double r2 = 1 / (v2x * v2x + v2y * v2y + v2z * v2z);
+      const double d12 = (v1x * v2x + v1y * v2y + v1z * v2z) * r2, d32 = (v3x * v2x + v3y * v2y + v3z * v2z) * r2;
+      v1x -= v2x * d12; v1y -= v2y * d12; v1z -= v2z * d12;
+      v3x -= v2x * d32; v3y -= v2y * d32; v3z -= v2z * d32;
+      const double cqd = (v1x * v3x + v1y * v3y + v1z * v3z) /
+                         sqrt((v1x * v1x + v1y * v1y + v1z * v1z) * (v3x * v3x + v3y * v3y + v3z * v3z));
+      e += (((double)c.w / 3 * cqd + (double)c.z / 2) * cqd + c.y) * cqd + c.x;
+    }
   }
   if (EV) {
     p.emol[m] = e;
@@ -275,6 +343,7 @@ int pair_enqueue(nnpe_ctx* c, bool ev) {
   const int N = c->natom;
   PairParams p;
   p.pos = c->d_pos; p.list = c->d_list; p.ncount = c->d_ncount; p.info = c->d_info; p.table = c->d_table;
+  p.gowner = c->d_gowner; p.gshift = c->d_gshift; p.g = c->grid;
   p.pairtype = c->d_pairtype; p.frc = c->d_frc; p.eatom = c->d_eatom; p.watom = c->d_watom;
   p.N = N; p.cap = c->cap; p.ntype = c->ntype; p.nbin = c->nbin;
   p.cutoff = c->pair_cutoff; p.cutsq = c->pair_cutoff * c->pair_cutoff;

@@ -80,7 +80,8 @@ class Restated:
         for k, m in enumerate(sysm.moltypes):
             spec[k, :m.n_atom, :m.n_atom] = m.special()
         amt = sysm.mol_type[mol_id]
-        self.h = self.lib.orc_create(sysm.natom, sysm.ntype, float(sysm.bl), _i32(sysm.typ), _f32(sysm.q), _i32(mol_id),
+        # the reference reads BL with %f into a float (environ.cpp:42)
+        self.h = self.lib.orc_create(sysm.natom, sysm.ntype, float(np.float32(sysm.bl)), _i32(sysm.typ), _f32(sysm.q), _i32(mol_id),
                                      _i32(intra), _i32(amt), len(sysm.moltypes), nmax, spec.ravel())
 
     def __del__(self):

@@ -78,7 +78,7 @@ def test_restated_mixture_gr_and_sq():
     cnt = o.gr_counts(15, 2, 1000, 10)
     np.testing.assert_array_equal(cnt, gm["gr_counts"])
     # S(q) of the reference's float g(r): FP64 transform agrees with its float transform
-    sq, qq = orc.sq(s.natom, s.bl, gm["gr_f32"].astype(np.float64), np.float32(10) / np.float32(1000), 512, 20.0)
+    sq, qq = orc.sq(s.natom, float(np.float32(s.bl)), gm["gr_f32"].astype(np.float64), np.float32(10) / np.float32(1000), 512, 20.0)
     np.testing.assert_allclose(qq, gm["qq"], rtol=1e-6)
     scale = np.abs(gm["sq_f32"]).max()
     assert np.abs(sq - gm["sq_f32"]).max() < 1e-3 * scale

@@ -114,7 +114,7 @@ def test_mixture_gr_counts_and_sq():
     np.testing.assert_allclose(gr, gm["gr_f32"], rtol=2e-6, atol=2e-6)
     # FP64 S(q) vs the FP64 transform of the same g(r) in the oracle, and vs the reference's float S(q)
     sq, q = e.sq(False)
-    sq_o, qq = orc.sq(s.natom, s.bl, gr, np.float32(10) / np.float32(1000), 512, 20.0)
+    sq_o, qq = orc.sq(s.natom, float(np.float32(s.bl)), gr, np.float32(10) / np.float32(1000), 512, 20.0)
     np.testing.assert_allclose(q, qq, rtol=1e-12)
     assert np.abs(sq - sq_o).max() < 1e-9 * np.abs(sq_o).max()
     assert np.abs(sq - gm["sq_f32"]).max() < 1e-3 * np.abs(gm["sq_f32"]).max()
