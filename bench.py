@@ -141,6 +141,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="water96k-classical", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--exact", action="store_true", help="pair forces in the reference's exact float sequence")
     ap.add_argument("--cpu-steps", type=int, default=10)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
@@ -172,6 +174,7 @@ def main():
 
     s, table = build_system(wl)
     e = make_engine(s, table, local)
+    e.pair_exact(args.exact)
     stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
     # untimed equilibration from the lattice start (Andersen, 300 K), then NVE at dt=0.5 fs
     e.verlet(1.0, True)

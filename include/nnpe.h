@@ -91,6 +91,9 @@ int nnpe_pair_set_table(nnpe_ctx* ctx, int nbin, const float* force, const float
 int nnpe_pair_load_table(nnpe_ctx* ctx, int nbin, const char* potfile);
 int nnpe_pair_get_table(nnpe_ctx* ctx, float* force, float* potential);
 int nnpe_pair_enable(nnpe_ctx* ctx, int on);
+/* on=1: fpair per pair in the reference's exact float sequence (IEEE sqrt/division, no FMA),
+ * bit-identical to pair.cpp:334-357; on=0 (default): same cutoff test and table, rsqrt + FMA. */
+int nnpe_pair_exact(nnpe_ctx* ctx, int on);
 
 /* ---- bonded terms (BOND/ANGLE/DIHEDRAL, bond.h:6-21, angle.h:6-21, dihedral.h:4-17) ----
  * Terms in atom ids (as autoGenerate expands them, bond.cpp:66-86); coefficients in the
@@ -162,6 +165,28 @@ int nnpe_run(nnpe_ctx* ctx, int nsteps, int log_interval, nnpe_thermo* log, int 
 /* Same loop with all device work of each step captured once in a CUDA graph and replayed;
  * the rebuild decision stays on the device. */
 int nnpe_run_graph(nnpe_ctx* ctx, int nsteps, int log_interval, nnpe_thermo* log, int max_log, int* nlog);
+
+/* ---- network term (NNPOTENTIAL_TBL, pair_nnp.h:54-75) -----------------------------------
+ * kind 0: the reference's tabulated NNP (20 Gaussian descriptors per special class from
+ *   coef_w/coef_d/coef_r [npair][4][20], pair part from coef_p [npair][4][6]; tables generated as
+ *   in the NNPOTENTIAL_TBL constructor, pair_nnp.cpp:521-590); e1/e2/scale/embw unused.
+ * kind 1: radial embedding 1->e1->e2 (tanh) per neighbour species (e1=32), times the cutoff
+ *   factor and `scale`, in descriptor slots s*e2+c (din=4*e2); coef_p may be NULL (no pair part).
+ * fitw: per species A1[din][h1] c1[h1] A2[h1][h2] c2[h2] A3[h2] c3 (tanh hidden layers).
+ * The network shares the pair list: cutoff <= pair_cutoff+skin. */
+int nnpe_nnp_set(nnpe_ctx* ctx, int kind, double cutoff, int nbin, double scale, int e1, int e2, int h1, int h2,
+                 const float* coef_p, const float* coef_w, const float* coef_d, const float* coef_r,
+                 const float* embw, const float* fitw);
+/* Reads the reference's NNP inputs: the paramfile (its first token names an NNPE model file:
+ * text header, "end", float32 weights) and the reference-format weight file (bond/angle/dihedral
+ * coefficients, coef_p, coef_w, coef_d, coef_r, pair_nnp.cpp:505-519), which, as in the reference,
+ * also sets the bonded coefficients. */
+int nnpe_nnp_load(nnpe_ctx* ctx, double cutoff, int nbin, const char* paramfile, const char* wtfile);
+/* 0: FP32 on CUDA cores (the plain form); 1: BF16 operands on tcgen05 tensor cores, FP32 accumulate. */
+int nnpe_nnp_precision(nnpe_ctx* ctx, int bf16);
+/* Descriptor G, dE/dG (atom-id order, [natom][din]) and per-atom network energy of the last evaluation. */
+int nnpe_nnp_get(nnpe_ctx* ctx, float* G, float* dEdG, double* e_atom);
+int nnpe_nnp_info(nnpe_ctx* ctx, int* din, int* kind);
 
 /* ---- profiling ------------------------------------------------------------------------
  * Enqueue one kernel class without synchronising (for event timing): 0 pair force, 1 list

@@ -44,6 +44,7 @@ _SIGS = {
     "nnpe_pair_load_table": (C.c_int, [_vp, C.c_int, C.c_char_p]),
     "nnpe_pair_get_table": (C.c_int, [_vp, _f32p, _f32p]),
     "nnpe_pair_enable": (C.c_int, [_vp, C.c_int]),
+    "nnpe_pair_exact": (C.c_int, [_vp, C.c_int]),
     "nnpe_bond_coef": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, _f32p]),
     "nnpe_angle_coef": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, _f32p]),
     "nnpe_dihedral_coef": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, _f32p]),
@@ -67,6 +68,13 @@ _SIGS = {
     "nnpe_get_atom_energy": (C.c_int, [_vp, _f64p]),
     "nnpe_run": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(Thermo), C.c_int, C.POINTER(C.c_int)]),
     "nnpe_run_graph": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(Thermo), C.c_int, C.POINTER(C.c_int)]),
+    "nnpe_nnp_set": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                               _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nnpe_nnp_load": (C.c_int, [_vp, C.c_double, C.c_int, C.c_char_p, C.c_char_p]),
+    "nnpe_nnp_precision": (C.c_int, [_vp, C.c_int]),
+    "nnpe_nnp_get": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "nnpe_nnp_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "nnpe_bonded_autogen": (C.c_int, [_vp, C.c_int, _f32p, C.c_int, _f32p, C.c_int, _f32p]),
     "nnpe_profile_enqueue": (C.c_int, [_vp, C.c_int]),
     "nnpe_launches_per_step": (C.c_int, [_vp]),
     "nnpe_gr_setup": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int]),

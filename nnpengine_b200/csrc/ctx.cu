@@ -371,6 +371,13 @@ int nnpe_pair_get_table(nnpe_ctx* c, float* force, float* potential) {
   return NNPE_OK;
 }
 
+int nnpe_pair_exact(nnpe_ctx* c, int on) {
+  if (!c) return NNPE_EARG;
+  c->exact_forces = on != 0;
+  c->graph_valid = false;
+  return NNPE_OK;
+}
+
 int nnpe_pair_enable(nnpe_ctx* c, int on) {
   if (!c) return NNPE_EARG;
   c->pair_on = on != 0;
@@ -456,7 +463,23 @@ int nnpe_bonded_set(nnpe_ctx* c, int nbond, const int* bonds, int nbtyp, const f
   TRY(up(&c->d_bcoef, bcoef, bcoef ? nbtyp : 0));
   TRY(up(&c->d_acoef, acoef, acoef ? natyp : 0));
   TRY(up(&c->d_dcoef, dcoef, dcoef ? ndtyp : 0));
+  c->nbtyp = nbtyp; c->natyp = natyp; c->ndtyp = ndtyp;
   c->graph_valid = false;
+  return NNPE_OK;
+}
+
+// Replace the bonded coefficients (stored form) keeping the topology.
+int nnpe_bonded_coefs(nnpe_ctx* c, const float* bcoef, const float* acoef, const float* dcoef) {
+  auto up = [&](float4* d, const float* h, int n) -> int {
+    if (n <= 0 || !d) return 0;
+    std::vector<float4> v(n);
+    for (int i = 0; i < n; ++i) v[i] = make_float4(h[4 * i], h[4 * i + 1], h[4 * i + 2], h[4 * i + 3]);
+    NNPE_CUDA(c, cudaMemcpy(d, v.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    return 0;
+  };
+  TRY(up(c->d_bcoef, bcoef, c->nbtyp));
+  TRY(up(c->d_acoef, acoef, c->natyp));
+  TRY(up(c->d_dcoef, dcoef, c->ndtyp));
   return NNPE_OK;
 }
 

@@ -67,7 +67,10 @@ __device__ __forceinline__ void pair_energy64(const PairParams& p, const float2*
   *w += 0.5 * fpair * rsq;
 }
 
-template <bool EV>
+// EXACT=true evaluates fpair with the reference's float sequence (IEEE sqrt and divisions, no
+// contraction), bit-identical per pair. EXACT=false keeps the same cutoff test (so the same pairs
+// interact) but uses rsqrt and fused multiply-adds: ~1 ulp per pair, forces within 1e-6 relative.
+template <bool EV, bool EXACT>
 __global__ void __launch_bounds__(128) k_pair(PairParams p) {
   const int lane = threadIdx.x & 31;
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -87,17 +90,31 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
     const float rsq = dx * dx + dy * dy + dz * dz;
     if (rsq < p.cutsq) {
       const int tj = (ent >> 27) & 7, s = ent >> 30;
-      const float r = sqrtf(rsq);
-      float ipw1 = r * p.r_dr - 0.5F;
-      const int t1 = (int)ipw1;
-      const float ipw2 = ipw1 - (float)t1;
-      ipw1 = 1 - ipw2;
       const float2* tab = p.table + (size_t)ptrow[tj] * (p.nbin + 1);
-      const float2 a = __ldg(tab + t1), b = __ldg(tab + t1 + 1);
-      float fpair = (a.x * ipw1 + b.x * ipw2) * c_special_lj[s];
-      const float qq = xi.w * xj.w * kElectricK;
-      fpair += qq * (1 / (r * rsq) + p.fc / r) * c_special_coul[s];
-      fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+      float fpair;
+      if (EXACT) {
+        const float r = sqrtf(rsq);
+        float ipw1 = r * p.r_dr - 0.5F;
+        const int t1 = (int)ipw1;
+        const float ipw2 = ipw1 - (float)t1;
+        ipw1 = 1 - ipw2;
+        const float2 a = __ldg(tab + t1), b = __ldg(tab + t1 + 1);
+        fpair = (a.x * ipw1 + b.x * ipw2) * c_special_lj[s];
+        const float qq = xi.w * xj.w * kElectricK;
+        fpair += qq * (1 / (r * rsq) + p.fc / r) * c_special_coul[s];
+      } else {
+        const float rinv = rsqrtf(rsq);
+        const float r = rsq * rinv;
+        const float u = fmaf(r, p.r_dr, -0.5F);
+        const int t1 = (int)u;
+        const float w2 = u - (float)t1;
+        const float2 a = __ldg(tab + t1), b = __ldg(tab + t1 + 1);
+        const float flj = fmaf(b.x - a.x, w2, a.x);
+        const float qq = xi.w * xj.w * kElectricK;
+        const float fco = qq * rinv * fmaf(rinv, rinv, p.fc);
+        fpair = fmaf(flj, c_special_lj[s], fco * c_special_coul[s]);
+      }
+      fx = fmaf(dx, fpair, fx); fy = fmaf(dy, fpair, fy); fz = fmaf(dz, fpair, fz);
     }
     if (EV) {
       const double3 xjd = exact_pos(p, j);
@@ -351,8 +368,13 @@ int pair_enqueue(nnpe_ctx* c, bool ev) {
   p.vc = -1 / p.cutoff; p.fc = p.vc / p.cutoff;  // pair.cpp:191-193 (erfc disabled)
   p.accumulate = false;
   const int blocks = nblocks((long)N * 32, 128);
-  if (ev) k_pair<true><<<blocks, 128, 0, c->stream>>>(p);
-  else k_pair<false><<<blocks, 128, 0, c->stream>>>(p);
+  if (c->exact_forces) {
+    if (ev) k_pair<true, true><<<blocks, 128, 0, c->stream>>>(p);
+    else k_pair<false, true><<<blocks, 128, 0, c->stream>>>(p);
+  } else {
+    if (ev) k_pair<true, false><<<blocks, 128, 0, c->stream>>>(p);
+    else k_pair<false, false><<<blocks, 128, 0, c->stream>>>(p);
+  }
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

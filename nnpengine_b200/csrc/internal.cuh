@@ -73,9 +73,11 @@ struct nnpe_ctx {
   // ---- pair table ----
   int nbin = 0;
   bool pair_on = true;
+  bool exact_forces = false;   // pair fpair in the reference's exact float sequence
   float2* d_table = nullptr;   // [npair][nbin+1] (F/r, U)
   // ---- bonded ----
   int nbond = 0, nangle = 0, ndih = 0;
+  int nbtyp = 0, natyp = 0, ndtyp = 0;
   int4* d_bond = nullptr;      // per term: type, atoms (atom ids)
   int4* d_angle = nullptr;
   int* d_dih = nullptr;        // 5 ints per term
@@ -210,4 +212,5 @@ int gr_tally_enqueue(nnpe_ctx* c, int inner);
 int alloc_state(nnpe_ctx* c);
 int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
 int nnp_forces_enqueue(nnpe_ctx* c, bool ev);
+int nnpe_bonded_coefs(nnpe_ctx* c, const float* bcoef, const float* acoef, const float* dcoef);
 void nnp_free(nnpe_ctx* c);

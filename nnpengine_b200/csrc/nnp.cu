@@ -1,13 +1,732 @@
-// Network term (NNPOTENTIAL_TBL, pair_nnp.cpp:433-793, and the radial-embedding network).
-#include "internal.cuh"
+// Network term: NNPOTENTIAL_TBL (pair_nnp.cpp:433-793) and the radial-embedding network.
+//
+// Two descriptor kinds share one pipeline (computeDescriptor -> nnEval -> compute, the call
+// sequence of run.cpp:1234-1249):
+//  * gauss: the reference's tabulated NNP. Tables tbl_pair/tbl_f_pair [npair][4][nbin+1] and
+//    tbl_desc/tbl_f_desc [npair][80][nbin+1] are generated on the host with the reference's float
+//    arithmetic (pair_nnp.cpp:521-590); 20 descriptor slots per atom, the special class selecting
+//    which 20 functions a pair adds (pair_nnp.cpp:663-683).
+//  * embed: per neighbour species an embedding net u=r/rc -> e1 -> e2 (tanh), times the
+//    reference's cutoff factor cff(r) and a descriptor scale, accumulated into slot s*e2+c.
+// Both feed a per-species fitting network din -> h1 -> h2 -> 1 (tanh) whose hand-written backward
+// gives dE/dG; forces are the reference's back-projection
+// fpair = f_pair(r) + sum_c (dE/dG_i + dE/dG_j)[c] f_desc_c(r),  F_i += fpair (x_i - x_j).
+//
+// Work split: a compact per-step list of the pairs inside the network cutoff (exact float test as
+// the reference's rsq<cutsq, pair_nnp.cpp:656) is filtered from the Verlet list; descriptor and
+// force kernels run one warp per atom over it (no atomics); the fitting network runs as tiled
+// GEMMs per species. precision 0 = FP32 on CUDA cores; precision 1 = BF16 tcgen05 (nnp_tc.cu).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
 
-struct NnpModel {
-  int dummy;
-};
+#include "internal.cuh"
+#include "nnp.cuh"
+
+// ---------------------------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+static int nalloc(nnpe_ctx* c, T** p, size_t n) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  NNPE_CUDA(c, cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)));
+  return 0;
+}
+template <typename T>
+static void nfree(T** p) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+}
 
 void nnp_free(nnpe_ctx* c) {
-  delete c->nnp;
+  NnpModel* m = c->nnp;
+  if (!m) return;
+  nfree(&m->d_embw); nfree(&m->d_fitw); nfree(&m->d_tdesc); nfree(&m->d_tpair); nfree(&m->d_G); nfree(&m->d_dG);
+  nfree(&m->d_enet); nfree(&m->d_list6); nfree(&m->d_n6); nfree(&m->d_sidx); nfree(&m->d_scount);
+  nfree(&m->d_H1); nfree(&m->d_G2); nfree(&m->d_G1); nfree(&m->d_soff_dev);
+  nnp_tc_free(m);
+  delete m;
   c->nnp = nullptr;
 }
-int nnp_forces_enqueue(nnpe_ctx*, bool) { return 0; }
-const double* nnp_atom_energy_ptr(nnpe_ctx*) { return nullptr; }
+
+const double* nnp_atom_energy_ptr(nnpe_ctx* c) { return c->nnp ? c->nnp->d_enet : nullptr; }
+
+// pair_nnp.cpp:521-590 in the reference's float arithmetic (exp is the C library's float exp).
+static void gen_tables(int npair, float cutoff, int nbin, const float* coef_p_in, const float* coef_w,
+                       const float* coef_d, const float* coef_r, std::vector<float2>& tpair, std::vector<float2>& tdesc) {
+  const int szd = 80, nb1 = nbin + 1;
+  tpair.assign((size_t)npair * 4 * nb1, make_float2(0, 0));
+  tdesc.assign((size_t)npair * szd * nb1, make_float2(0, 0));
+  std::vector<float> cp(coef_p_in, coef_p_in + (size_t)npair * 24);
+  const float dr = cutoff / nbin;
+  auto sqr = [](float a) { return a * a; };
+  for (int p = 0; p < npair; ++p) {
+    for (int k = 0; k < 4; ++k) {
+      float* q = cp.data() + p * 24 + k * 6;
+      float src2 = sqr(q[1] / cutoff), src6 = src2 * src2 * src2;
+      const float elim = -2 * q[5] / cutoff - q[0] * src6 * (-7 + src2 * (9 * q[2] + src2 * (11 * q[3] + src2 * 13 * q[4])));
+      const float flim = (q[5] / cutoff + q[0] * src6 * (-6 + src2 * ((q[2] *= 8) + src2 * ((q[3] *= 10) + src2 * (q[4] *= 12))))) / cutoff;
+      q[1] *= q[1];
+      float2* t = tpair.data() + ((size_t)p * 4 + k) * nb1;
+      for (int i = 0; i < nbin; ++i) {
+        float rr, rsq;
+        rsq = sqr(rr = dr * (i + 0.5));
+        src2 = q[1] / rsq;
+        src6 = src2 * src2 * src2;
+        const float f = (q[5] / rr + (*q) * src6 * (-6 + src2 * (q[2] + src2 * (q[3] + src2 * q[4])))) / rsq - (flim) / rr;
+        const float u = q[5] / rr + (*q) * src6 * (-1 + src2 * (q[2] * .125F + src2 * (q[3] * .1F + src2 * q[4] * .08333333333333333333F))) +
+                        (flim) * rr + elim;
+        t[i] = make_float2(u, f);   // (U, F/r)
+      }
+      t[nbin] = make_float2(0, 0);
+    }
+    const float *w = coef_w + (size_t)p * szd, *d = coef_d + (size_t)p * szd, *r0 = coef_r + (size_t)p * szd;
+    for (int i = 0; i < nbin; ++i) {
+      float rr = dr * (i + 0.5), cf2, rrcsq_1, cff, cfr;
+      rrcsq_1 = 1 + sqr(cf2 = rr - cutoff);
+      cfr = (-2 * (cff = 1 - 1 / rrcsq_1)) / rr;
+      cf2 /= (-.5f * rr * sqr(rrcsq_1));
+      for (int k = 0; k < szd; ++k) {
+        const float rr0 = rr - r0[k];
+        const float drr0 = d[k] * rr0;
+        const float wexp = std::exp(drr0 * rr0) * w[k];
+        tdesc[((size_t)p * szd + k) * nb1 + i] = make_float2(wexp * cff, wexp * (cf2 + drr0 * cfr));   // (desc, f_desc)
+      }
+    }
+  }
+}
+
+static size_t fit_block(int din, int h1, int h2) { return (size_t)din * h1 + h1 + (size_t)h1 * h2 + h2 + h2 + 1; }
+
+int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, int e1, int e2, int h1, int h2,
+                 const float* coef_p, const float* coef_w, const float* coef_d, const float* coef_r, const float* embw,
+                 const float* fitw) {
+  if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: call nnpe_setup first");
+  if ((kind != 0 && kind != 1) || !(cutoff > 0) || h1 <= 0 || h2 <= 0 || h1 > 256 || h2 > 256 || !fitw)
+    return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: bad network shape");
+  if ((float)cutoff > c->pair_cutoff + c->skin) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: network cutoff beyond the list");
+  if (kind == 1 && (e1 != 32 || e2 <= 0 || e2 > 64 || !embw)) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: embedding must be 1->32->e2 (e2<=64)");
+  if (kind == 0 && (nbin <= 0 || !coef_p || !coef_w || !coef_d || !coef_r)) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: tables need coefficients");
+  cudaSetDevice(c->device);
+  nnp_free(c);
+  auto* m = new NnpModel();
+  c->nnp = m;
+  m->kind = kind; m->rc = (float)cutoff; m->nbin = nbin; m->scale = (float)scale; m->e1 = e1; m->e2 = e2;
+  m->din = kind == 0 ? 20 : 4 * e2; m->h1 = h1; m->h2 = h2; m->ntype = c->ntype; m->npair = c->npair;
+  m->cap6 = 256;
+  const int N = c->natom;
+  int rc = 0;
+  if (kind == 0) {
+    std::vector<float2> tp, td;
+    gen_tables(c->npair, m->rc, nbin, coef_p, coef_w, coef_d, coef_r, tp, td);
+    if ((rc = nalloc(c, &m->d_tpair, tp.size())) || (rc = nalloc(c, &m->d_tdesc, td.size()))) return rc;
+    NNPE_CUDA(c, cudaMemcpy(m->d_tpair, tp.data(), sizeof(float2) * tp.size(), cudaMemcpyHostToDevice));
+    NNPE_CUDA(c, cudaMemcpy(m->d_tdesc, td.data(), sizeof(float2) * td.size(), cudaMemcpyHostToDevice));
+    m->h_tpair = tp;
+  } else {
+    const size_t eb = (size_t)e1 + e1 + (size_t)e1 * e2 + e2;
+    if ((rc = nalloc(c, &m->d_embw, eb * c->ntype))) return rc;
+    NNPE_CUDA(c, cudaMemcpy(m->d_embw, embw, sizeof(float) * eb * c->ntype, cudaMemcpyHostToDevice));
+    m->h_embw.assign(embw, embw + eb * c->ntype);
+  }
+  const size_t fb = fit_block(m->din, h1, h2);
+  if ((rc = nalloc(c, &m->d_fitw, fb * c->ntype))) return rc;
+  NNPE_CUDA(c, cudaMemcpy(m->d_fitw, fitw, sizeof(float) * fb * c->ntype, cudaMemcpyHostToDevice));
+  m->h_fitw.assign(fitw, fitw + fb * c->ntype);
+  if ((rc = nalloc(c, &m->d_G, (size_t)N * m->din)) || (rc = nalloc(c, &m->d_dG, (size_t)N * m->din)) ||
+      (rc = nalloc(c, &m->d_enet, N)) || (rc = nalloc(c, &m->d_list6, (size_t)N * m->cap6)) ||
+      (rc = nalloc(c, &m->d_n6, N)) || (rc = nalloc(c, &m->d_sidx, N)) || (rc = nalloc(c, &m->d_scount, NNPE_MAX_TYPES)) ||
+      (rc = nalloc(c, &m->d_H1, (size_t)N * h1)) || (rc = nalloc(c, &m->d_G2, (size_t)N * h2)) ||
+      (rc = nalloc(c, &m->d_G1, (size_t)N * h1)))
+    return rc;
+  NNPE_CUDA(c, cudaMemset(m->d_enet, 0, sizeof(double) * N));
+  NNPE_CUDA(c, cudaMemset(m->d_n6, 0, sizeof(int) * N));
+  // species offsets are fixed (type counts); membership follows the sort
+  m->soff.assign(c->ntype + 1, 0);
+  std::vector<int> cnt(c->ntype, 0);
+  for (int t : c->h_typ) ++cnt[t];
+  for (int t = 0; t < c->ntype; ++t) m->soff[t + 1] = m->soff[t] + cnt[t];
+  c->graph_valid = false;
+  return nnp_tc_setup(c);
+}
+
+int nnpe_nnp_precision(nnpe_ctx* c, int bf16) {
+  if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_precision: no network");
+  if (bf16 && c->nnp->kind != 1) return nnpe_fail(c, NNPE_EARG, "BF16 tensor-core path is for the embedding network");
+  c->nnp->bf16 = bf16 != 0;
+  c->graph_valid = false;
+  return NNPE_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+// Pairs inside the network cutoff, in list order, with the reference's float test rsq<cutsq.
+__global__ void __launch_bounds__(128) k_filter6(const float4* __restrict__ pos, const uint32_t* __restrict__ list,
+                                                 const int* __restrict__ ncount, int cap, uint32_t* __restrict__ list6,
+                                                 int* __restrict__ n6, int cap6, float cutsq, int N, int* ctrl) {
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= N) return;
+  const float4 xi = pos[i];
+  const uint32_t* row = list + (size_t)i * cap;
+  uint32_t* out = list6 + (size_t)i * cap6;
+  const int n = ncount[i];
+  int cnt = 0;
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    bool ok = false;
+    uint32_t e = 0;
+    if (k < n) {
+      e = row[k];
+      const float4 xj = pos[e & NNPE_J_MASK];
+      ok = rsq3(fsub(xi.x, xj.x), fsub(xi.y, xj.y), fsub(xi.z, xj.z)) < cutsq;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (ok) {
+      const int idx = cnt + __popc(b & ((1u << lane) - 1));
+      if (idx < cap6) out[idx] = e;
+    }
+    cnt += __popc(b);
+  }
+  if (lane == 0) {
+    n6[i] = min(cnt, cap6);
+    if (cnt > cap6) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_LIST_OVERFLOW);
+  }
+}
+
+// Species membership lists (sorted atom indices grouped by type) for the per-species fitting net.
+__global__ void k_species(const int2* __restrict__ info, int* __restrict__ sidx, int* __restrict__ scount,
+                          const int* __restrict__ soff, int N) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int t = info[i].y & 0xFF;
+  sidx[soff[t] + atomicAdd(&scount[t], 1)] = i;
+}
+
+__device__ __forceinline__ int owner_of(int j, int N, const int* __restrict__ gowner) { return j < N ? j : gowner[j - N]; }
+
+// ---- gauss (tabulated) descriptor: computeDescriptor (pair_nnp.cpp:625-688) ----
+__global__ void __launch_bounds__(128) k_gauss_desc(NnpArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= a.N) return;
+  const float4 xi = a.pos[i];
+  const int* ptrow = a.pairtype + (a.info[i].y & 0xFF) * a.ntype;
+  const uint32_t* row = a.list6 + (size_t)i * a.cap6;
+  const int n = a.n6[i];
+  float acc[20];
+#pragma unroll
+  for (int k = 0; k < 20; ++k) acc[k] = 0.f;
+  const int nb1 = a.nbin + 1;
+  for (int k = lane; k < n; k += 32) {
+    const uint32_t e = row[k];
+    const float4 xj = a.pos[e & NNPE_J_MASK];
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+    float ipw1 = r * a.r_dr - 0.5F;
+    const int t1 = (int)ipw1;
+    const float ipw2 = ipw1 - (float)t1;
+    ipw1 = 1 - ipw2;
+    const int s = e >> 30, p = ptrow[(e >> 27) & 7];
+    const float2* t = a.tdesc + ((size_t)p * 80 + 20 * s) * nb1 + t1;
+#pragma unroll
+    for (int c = 0; c < 20; ++c) {
+      const float2 u = __ldg(t + (size_t)c * nb1), v = __ldg(t + (size_t)c * nb1 + 1);
+      acc[c] += u.x * ipw1 + v.x * ipw2;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 20; ++c) {
+    float v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[c] = v;
+  }
+  if (lane < 20) {
+    float v = 0.f;
+#pragma unroll
+    for (int c = 0; c < 20; ++c) v = lane == c ? acc[c] : v;
+    a.G[(size_t)i * 20 + lane] = v;
+  }
+}
+
+// ---- gauss force: NNPOTENTIAL_TBL::compute<ev> (pair_nnp.cpp:710-793) ----
+template <bool EV>
+__global__ void __launch_bounds__(128) k_gauss_force(NnpArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= a.N) return;
+  const float4 xi = a.pos[i];
+  const int* ptrow = a.pairtype + (a.info[i].y & 0xFF) * a.ntype;
+  const uint32_t* row = a.list6 + (size_t)i * a.cap6;
+  const int n = a.n6[i];
+  const float* dGi = a.dG + (size_t)i * 20;
+  const int nb1 = a.nbin + 1;
+  float fx = 0, fy = 0, fz = 0;
+  double e = 0, w = 0;
+  for (int k = lane; k < n; k += 32) {
+    const uint32_t ent = row[k];
+    const int j = ent & NNPE_J_MASK;
+    const float4 xj = a.pos[j];
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float rsq = dx * dx + dy * dy + dz * dz;
+    const float r = sqrtf(rsq);
+    float ipw1 = r * a.r_dr - 0.5F;
+    const int t1 = (int)ipw1;
+    const float ipw2 = ipw1 - (float)t1;
+    ipw1 = 1 - ipw2;
+    const int s = ent >> 30, p = ptrow[(ent >> 27) & 7];
+    const float2* tp = a.tpair + ((size_t)p * 4 + s) * nb1 + t1;
+    const float2 pa = __ldg(tp), pb = __ldg(tp + 1);
+    float fpair = pa.y * ipw1 + pb.y * ipw2;
+    const float* dGj = a.dG + (size_t)owner_of(j, a.N, a.gowner) * 20;
+    const float2* t = a.tdesc + ((size_t)p * 80 + 20 * s) * nb1 + t1;
+#pragma unroll 4
+    for (int c = 0; c < 20; ++c) {
+      const float2 u = __ldg(t + (size_t)c * nb1), v = __ldg(t + (size_t)c * nb1 + 1);
+      fpair += (dGi[c] + dGj[c]) * (u.y * ipw1 + v.y * ipw2);
+    }
+    fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+    if (EV) {
+      e += 0.5 * (double)(pa.x * ipw1 + pb.x * ipw2);
+      w += 0.5 * (double)(fpair * rsq);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    if (EV) {
+      e += __shfl_xor_sync(0xffffffffu, e, o);
+      w += __shfl_xor_sync(0xffffffffu, w, o);
+    }
+  }
+  if (lane == 0) {
+    const float4 f = a.frc[i];
+    a.frc[i] = make_float4(f.x + fx, f.y + fy, f.z + fz, f.w);
+    if (EV) { a.eatom[i] += e; a.watom[i] += w; }
+  }
+}
+
+// ---- embedding descriptor (FP32): one warp per atom, lanes over pairs; each lane evaluates its
+// pair's e1->e2 embedding with the weights of the neighbour's species from shared memory, then
+// the warp reduces channel sums per special class through shared memory (deterministic order).
+constexpr int kEmbWarps = 4;
+__global__ void __launch_bounds__(kEmbWarps * 32) k_emb_desc_f32(NnpArgs a) {
+  extern __shared__ float sm[];
+  const int E1 = 32, E2 = a.e2;
+  const size_t eb = (size_t)E1 + E1 + (size_t)E1 * E2 + E2;
+  float* W = sm;                                   // [ntype][eb]
+  float* Y = sm + eb * a.ntype;                    // [warps][32][E2+1]
+  int* S = (int*)(Y + kEmbWarps * 32 * (E2 + 1));  // [warps][32]
+  for (int k = threadIdx.x; k < (int)(eb * a.ntype); k += blockDim.x) W[k] = a.embw[k];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int i = blockIdx.x * kEmbWarps + wi;
+  if (i >= a.N) return;
+  float* Yw = Y + wi * 32 * (E2 + 1);
+  int* Sw = S + wi * 32;
+  const float4 xi = a.pos[i];
+  const uint32_t* row = a.list6 + (size_t)i * a.cap6;
+  const int n = a.n6[i];
+  float acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const float r_rc = 1.f / a.rc;
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    int s = 0;
+    if (k < n) {
+      const uint32_t ent = row[k];
+      const float4 xj = a.pos[ent & NNPE_J_MASK];
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+      const float u = r * r_rc, cf = r - a.rc, cff = a.scale * (1.f - 1.f / (1.f + cf * cf));
+      s = ent >> 30;
+      const float* w = W + eb * ((ent >> 27) & 7);
+      float h[32];
+#pragma unroll
+      for (int q = 0; q < 32; ++q) h[q] = tanhf(w[q] * u + w[32 + q]);
+      const float* W2 = w + 64;
+      const float* b2 = W2 + 32 * E2;
+      for (int cc = 0; cc < E2; ++cc) {
+        float z = b2[cc];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) z += h[q] * W2[q * E2 + cc];
+        Yw[lane * (E2 + 1) + cc] = tanhf(z) * cff;
+      }
+    } else {
+      for (int cc = 0; cc < E2; ++cc) Yw[lane * (E2 + 1) + cc] = 0.f;
+    }
+    Sw[lane] = s;
+    __syncwarp();
+    const int m = min(32, n - base);
+    for (int l = 0; l < m; ++l) {
+      const int sl = Sw[l];
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        const int cc = lane + 32 * h2;
+        const float v = cc < E2 ? Yw[l * (E2 + 1) + cc] : 0.f;
+        acc[0][h2] += sl == 0 ? v : 0.f;
+        acc[1][h2] += sl == 1 ? v : 0.f;
+        acc[2][h2] += sl == 2 ? v : 0.f;
+        acc[3][h2] += sl == 3 ? v : 0.f;
+      }
+    }
+    __syncwarp();
+  }
+  float* Gi = a.G + (size_t)i * 4 * E2;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int h2 = 0; h2 < 2; ++h2) {
+      const int cc = lane + 32 * h2;
+      if (cc < E2) Gi[s * E2 + cc] = acc[s][h2];
+    }
+}
+
+// ---- embedding force (FP32): recompute the pair's embedding, back-propagate
+// a_c = scale*(dE/dG_i + dE/dG_j)[s*e2+c] through it to dE/dr, fpair = -dE/dr / r.
+template <bool EV>
+__global__ void __launch_bounds__(kEmbWarps * 32) k_emb_force_f32(NnpArgs a) {
+  extern __shared__ float sm[];
+  const int E1 = 32, E2 = a.e2;
+  const size_t eb = (size_t)E1 + E1 + (size_t)E1 * E2 + E2;
+  float* W = sm;
+  for (int k = threadIdx.x; k < (int)(eb * a.ntype); k += blockDim.x) W[k] = a.embw[k];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int i = blockIdx.x * kEmbWarps + wi;
+  if (i >= a.N) return;
+  const float4 xi = a.pos[i];
+  const uint32_t* row = a.list6 + (size_t)i * a.cap6;
+  const int n = a.n6[i];
+  const float* dGi = a.dG + (size_t)i * 4 * E2;
+  const float r_rc = 1.f / a.rc;
+  float fx = 0, fy = 0, fz = 0;
+  double w = 0;
+  for (int k = lane; k < n; k += 32) {
+    const uint32_t ent = row[k];
+    const int j = ent & NNPE_J_MASK;
+    const float4 xj = a.pos[j];
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float rsq = dx * dx + dy * dy + dz * dz;
+    const float r = sqrtf(rsq);
+    const float u = r * r_rc, cf = r - a.rc, den = 1.f + cf * cf;
+    const float cff = 1.f - 1.f / den, dcff = 2.f * cf / (den * den);
+    const int s = ent >> 30;
+    const float* wt = W + eb * ((ent >> 27) & 7);
+    const float* dGj = a.dG + (size_t)owner_of(j, a.N, a.gowner) * 4 * E2 + s * E2;
+    const float* dGis = dGi + s * E2;
+    float h[32], t[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) { h[q] = tanhf(wt[q] * u + wt[32 + q]); t[q] = 0.f; }
+    const float* W2 = wt + 64;
+    const float* b2 = W2 + 32 * E2;
+    float dEdr = 0.f;
+    for (int cc = 0; cc < E2; ++cc) {
+      float z = b2[cc];
+#pragma unroll
+      for (int q = 0; q < 32; ++q) z += h[q] * W2[q * E2 + cc];
+      const float y = tanhf(z);
+      const float ac = a.scale * (dGis[cc] + dGj[cc]);
+      dEdr += ac * y * dcff;
+      const float g = ac * cff * (1.f - y * y);
+#pragma unroll
+      for (int q = 0; q < 32; ++q) t[q] += g * W2[q * E2 + cc];
+    }
+#pragma unroll
+    for (int q = 0; q < 32; ++q) dEdr += t[q] * (1.f - h[q] * h[q]) * wt[q] * r_rc;
+    const float fpair = -dEdr / r;
+    fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+    if (EV) w += 0.5 * (double)(fpair * rsq);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    if (EV) w += __shfl_xor_sync(0xffffffffu, w, o);
+  }
+  if (lane == 0) {
+    const float4 f = a.frc[i];
+    a.frc[i] = make_float4(f.x + fx, f.y + fy, f.z + fz, f.w);
+    if (EV) a.watom[i] += w;
+  }
+}
+
+// ---- fitting network (FP32): C[rows] = epi(A[rows] x B), 32 rows x 128 columns per block,
+// 256 threads with 4x4 outputs each, K staged through shared memory in chunks of 32.
+enum FitEpi { EPI_L1 = 0, EPI_L2 = 1, EPI_B2 = 2, EPI_B1 = 3 };
+struct FitArgs {
+  const float* A;      // [M x K] rows in species order (or gathered through idx)
+  const int* idx;      // row -> atom (gather/scatter), or null for direct rows
+  const float* B;      // weights
+  bool transB;         // B element (k,n) = transB ? B[n*K + k] : B[k*N + n]
+  int M, K, N;
+  const float* bias;   // [N]
+  const float* a3;     // L2: output weights [N]
+  const float* c3;     // L2: output bias
+  const float* aux;    // B2: H1 rows (for 1-h^2)
+  float* C;            // output rows
+  double* enet;        // L2: per-atom energy (indexed through idx)
+  bool gatherA, scatterC;
+};
+
+template <int EPI>
+__global__ void __launch_bounds__(256) k_fit_gemm(FitArgs f) {
+  __shared__ float As[32][33];
+  __shared__ float Bs[32][128 + 4];
+  const int t = threadIdx.x;
+  const int tr = t >> 5, tc = t & 31;       // rows tr*4..+4, cols tc*4..+4
+  const int row0 = blockIdx.x * 32, col0 = blockIdx.y * 128;
+  float acc[4][4] = {};
+  for (int k0 = 0; k0 < f.K; k0 += 32) {
+    for (int e = t; e < 32 * 32; e += 256) {
+      const int r = e >> 5, k = e & 31;
+      const int gr = row0 + r;
+      float v = 0.f;
+      if (gr < f.M && k0 + k < f.K) {
+        const int src = f.gatherA ? f.idx[gr] : gr;
+        v = f.A[(size_t)src * f.K + k0 + k];
+      }
+      As[r][k] = v;
+    }
+    for (int e = t; e < 32 * 128; e += 256) {
+      const int k = e >> 7, n = e & 127;
+      float v = 0.f;
+      if (k0 + k < f.K && col0 + n < f.N)
+        v = f.transB ? f.B[(size_t)(col0 + n) * f.K + k0 + k] : f.B[(size_t)(k0 + k) * f.N + col0 + n];
+      Bs[k][n] = v;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      float av[4], bv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) { av[q] = As[tr * 4 + q][k]; bv[q] = Bs[k][tc * 4 + q]; }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int p = 0; p < 4; ++p) acc[q][p] += av[q] * bv[p];
+    }
+    __syncthreads();
+  }
+  float epart[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int gr = row0 + tr * 4 + q;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int gc = col0 + tc * 4 + p;
+      if (gr >= f.M || gc >= f.N) continue;
+      float v = acc[q][p];
+      if (EPI == EPI_L1) {
+        v = tanhf(v + f.bias[gc]);
+        f.C[(size_t)gr * f.N + gc] = v;
+      } else if (EPI == EPI_L2) {
+        const float h = tanhf(v + f.bias[gc]);
+        epart[q] += h * f.a3[gc];
+        f.C[(size_t)gr * f.N + gc] = f.a3[gc] * (1.f - h * h);
+      } else if (EPI == EPI_B2) {
+        const float h = f.aux[(size_t)gr * f.N + gc];
+        f.C[(size_t)gr * f.N + gc] = v * (1.f - h * h);
+      } else {
+        f.C[(size_t)f.idx[gr] * f.N + gc] = v;
+      }
+    }
+  }
+  if (EPI == EPI_L2) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float v = epart[q];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      const int gr = row0 + tr * 4 + q;
+      if (tc == 0 && gr < f.M) f.enet[f.idx[gr]] = (double)v + (double)f.c3[0];
+    }
+  }
+}
+
+}  // namespace
+
+static NnpArgs make_args(nnpe_ctx* c) {
+  NnpModel* m = c->nnp;
+  NnpArgs a;
+  a.pos = c->d_pos; a.info = c->d_info; a.pairtype = c->d_pairtype; a.gowner = c->d_gowner; a.list6 = m->d_list6;
+  a.n6 = m->d_n6; a.cap6 = m->cap6; a.ntype = c->ntype; a.N = c->natom; a.nbin = m->nbin;
+  a.r_dr = m->kind == 0 ? (float)m->nbin / m->rc : 0.f;
+  a.rc = m->rc; a.scale = m->scale; a.e2 = m->e2; a.tdesc = m->d_tdesc; a.tpair = m->d_tpair; a.embw = m->d_embw;
+  a.G = m->d_G; a.dG = m->d_dG; a.frc = c->d_frc; a.eatom = c->d_eatom; a.watom = c->d_watom;
+  return a;
+}
+
+// Fitting network forward + backward: per species, 4 GEMMs (L1, L2 with energy, B2, B1).
+static int fit_f32_enqueue(nnpe_ctx* c) {
+  NnpModel* m = c->nnp;
+  const size_t fb = fit_block(m->din, m->h1, m->h2);
+  for (int t = 0; t < c->ntype; ++t) {
+    const int M = m->soff[t + 1] - m->soff[t];
+    if (!M) continue;
+    const float* w = m->d_fitw + fb * t;
+    const float *A1 = w, *c1 = A1 + (size_t)m->din * m->h1, *A2 = c1 + m->h1, *c2 = A2 + (size_t)m->h1 * m->h2;
+    const float *A3 = c2 + m->h2, *c3 = A3 + m->h2;
+    const int* idx = m->d_sidx + m->soff[t];
+    float* H1 = m->d_H1 + (size_t)m->soff[t] * m->h1;
+    float* G2 = m->d_G2 + (size_t)m->soff[t] * m->h2;
+    float* G1 = m->d_G1 + (size_t)m->soff[t] * m->h1;
+    FitArgs f{};
+    f.idx = idx; f.M = M;
+    dim3 g1(nblocks(M, 32), nblocks(m->h1, 128));
+    f.A = m->d_G; f.K = m->din; f.B = A1; f.N = m->h1; f.bias = c1; f.C = H1; f.gatherA = true; f.transB = false;
+    k_fit_gemm<EPI_L1><<<g1, 256, 0, c->stream>>>(f);
+    dim3 g2(nblocks(M, 32), nblocks(m->h2, 128));
+    f.A = H1; f.K = m->h1; f.B = A2; f.N = m->h2; f.bias = c2; f.C = G2; f.gatherA = false; f.a3 = A3; f.c3 = c3;
+    f.enet = m->d_enet;
+    k_fit_gemm<EPI_L2><<<g2, 256, 0, c->stream>>>(f);
+    dim3 g3(nblocks(M, 32), nblocks(m->h1, 128));
+    f.A = G2; f.K = m->h2; f.B = A2; f.N = m->h1; f.transB = true; f.aux = H1; f.C = G1;
+    k_fit_gemm<EPI_B2><<<g3, 256, 0, c->stream>>>(f);
+    dim3 g4(nblocks(M, 32), nblocks(m->din, 128));
+    f.A = G1; f.K = m->h1; f.B = A1; f.N = m->din; f.transB = true; f.C = m->d_dG;
+    k_fit_gemm<EPI_B1><<<g4, 256, 0, c->stream>>>(f);
+  }
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int nnp_species_enqueue(nnpe_ctx* c) {
+  NnpModel* m = c->nnp;
+  if (!m->d_soff_dev) NNPE_CUDA(c, cudaMalloc(&m->d_soff_dev, sizeof(int) * (NNPE_MAX_TYPES + 1)));
+  NNPE_CUDA(c, cudaMemcpyAsync(m->d_soff_dev, m->soff.data(), sizeof(int) * m->soff.size(), cudaMemcpyHostToDevice, c->stream));
+  NNPE_CUDA(c, cudaMemsetAsync(m->d_scount, 0, sizeof(int) * NNPE_MAX_TYPES, c->stream));
+  k_species<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_info, m->d_sidx, m->d_scount, m->d_soff_dev, c->natom);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int nnp_forces_enqueue(nnpe_ctx* c, bool ev) {
+  NnpModel* m = c->nnp;
+  const int N = c->natom;
+  cudaStream_t st = c->stream;
+  const float cs = m->rc * m->rc;
+  k_filter6<<<nblocks((long)N * 32, 128), 128, 0, st>>>(c->d_pos, c->d_list, c->d_ncount, c->cap, m->d_list6, m->d_n6,
+                                                      m->cap6, cs, N, c->d_ctrl);
+  if (int rc = nnp_species_enqueue(c)) return rc;
+  NnpArgs a = make_args(c);
+  if (m->bf16) return nnp_tc_forces_enqueue(c, ev);
+  if (m->kind == 0) {
+    k_gauss_desc<<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
+  } else {
+    const size_t eb = (size_t)32 + 32 + 32 * (size_t)m->e2 + m->e2;
+    const size_t smem = sizeof(float) * (eb * c->ntype + kEmbWarps * 32 * (m->e2 + 1)) + sizeof(int) * kEmbWarps * 32;
+    k_emb_desc_f32<<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
+  }
+  if (int rc = fit_f32_enqueue(c)) return rc;
+  if (m->kind == 0) {
+    if (ev) k_gauss_force<true><<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
+    else k_gauss_force<false><<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
+  } else {
+    const size_t eb = (size_t)32 + 32 + 32 * (size_t)m->e2 + m->e2;
+    const size_t smem = sizeof(float) * eb * c->ntype;
+    if (ev) k_emb_force_f32<true><<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
+    else k_emb_force_f32<false><<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
+  }
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+int nnpe_nnp_get(nnpe_ctx* c, float* G, float* dG, double* e_atom) {
+  if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_get: no network");
+  NnpModel* m = c->nnp;
+  const int N = c->natom, D = m->din;
+  std::vector<int> aid(N);
+  std::vector<float> g((size_t)N * D), d((size_t)N * D);
+  std::vector<double> e(N);
+  NNPE_CUDA(c, cudaMemcpyAsync(aid.data(), c->d_atom_id, sizeof(int) * N, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(g.data(), m->d_G, sizeof(float) * g.size(), cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(d.data(), m->d_dG, sizeof(float) * d.size(), cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(e.data(), m->d_enet, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < N; ++i) {
+    const int a = aid[i];
+    if (G) std::memcpy(G + (size_t)a * D, g.data() + (size_t)i * D, sizeof(float) * D);
+    if (dG) std::memcpy(dG + (size_t)a * D, d.data() + (size_t)i * D, sizeof(float) * D);
+    if (e_atom) e_atom[a] = e[i];
+  }
+  return NNPE_OK;
+}
+
+int nnpe_nnp_info(nnpe_ctx* c, int* din, int* kind) {
+  if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_info: no network");
+  if (din) *din = c->nnp->din;
+  if (kind) *kind = c->nnp->kind;
+  return NNPE_OK;
+}
+
+// NNPOTENTIAL_TBL constructor inputs (pair_nnp.cpp:457-519): the paramfile's first token names
+// the model file (here an NNPE model: text header up to "end", then float32 weights); the weight
+// file holds bond/angle/dihedral coefficients in their raw form (setParam() doubles the 2a/2c
+// entries and scales the dihedral ones, bond.cpp:57-64 etc.), then coef_p, coef_w, coef_d, coef_r.
+int nnpe_nnp_load(nnpe_ctx* c, double cutoff, int nbin, const char* paramfile, const char* wtfile) {
+  if (!c || !c->have_setup || !paramfile || !wtfile) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_load");
+  char model[512];
+  FILE* fp = fopen(paramfile, "r");
+  if (!fp) return nnpe_fail(c, NNPE_EFILE, std::string("cannot open ") + paramfile);
+  const int got = fscanf(fp, "%511s", model);
+  fclose(fp);
+  if (got != 1) return nnpe_fail(c, NNPE_EFILE, "paramfile: read error");
+  fp = fopen(model, "rb");
+  if (!fp) return nnpe_fail(c, NNPE_EFILE, std::string("cannot open model ") + model);
+  char line[512];
+  std::string desc;
+  int e1 = 32, e2 = 64, h1 = 0, h2 = 0, ntype = 0, ngauss = 20;
+  float scale = 1.f;
+  while (fgets(line, sizeof line, fp)) {
+    char key[64];
+    if (sscanf(line, "%63s", key) != 1) continue;
+    const std::string k(key);
+    if (k == "end") break;
+    if (k == "descriptor") {
+      char d[64];
+      int n = sscanf(line, "%*s %63s", d);
+      if (n != 1) { fclose(fp); return nnpe_fail(c, NNPE_EFILE, "model: descriptor line"); }
+      desc = d;
+      if (desc == "embed") sscanf(line, "%*s %*s %d %d %f", &e1, &e2, &scale);
+      else sscanf(line, "%*s %*s %d", &ngauss);
+    } else if (k == "fitting") sscanf(line, "%*s %d %d", &h1, &h2);
+    else if (k == "ntype") sscanf(line, "%*s %d", &ntype);
+  }
+  if ((desc != "embed" && desc != "gauss") || ntype != c->ntype || h1 <= 0 || h2 <= 0 || (desc == "gauss" && ngauss != 20)) {
+    fclose(fp);
+    return nnpe_fail(c, NNPE_EFILE, "model: unsupported header (descriptor embed|gauss 20, fitting h1 h2, ntype)");
+  }
+  const int kind = desc == "embed" ? 1 : 0;
+  const int din = kind ? 4 * e2 : 20;
+  const size_t eb = (size_t)e1 + e1 + (size_t)e1 * e2 + e2;
+  std::vector<float> embw(kind ? eb * ntype : 0), fitw(fit_block(din, h1, h2) * ntype);
+  if ((kind && fread(embw.data(), sizeof(float), embw.size(), fp) != embw.size()) ||
+      fread(fitw.data(), sizeof(float), fitw.size(), fp) != fitw.size()) {
+    fclose(fp);
+    return nnpe_fail(c, NNPE_EFILE, "model: truncated weights");
+  }
+  fclose(fp);
+  fp = fopen(wtfile, "rb");
+  if (!fp) return nnpe_fail(c, NNPE_EFILE, std::string("cannot open ") + wtfile);
+  const int P = c->npair;
+  std::vector<float> bc((size_t)c->nbtyp * 4), ac((size_t)c->natyp * 4), dc((size_t)c->ndtyp * 4), cp((size_t)P * 24),
+      cw((size_t)P * 80), cd((size_t)P * 80), cr((size_t)P * 80);
+  bool ok = fread(bc.data(), 4, bc.size(), fp) == bc.size() && fread(ac.data(), 4, ac.size(), fp) == ac.size() &&
+            fread(dc.data(), 4, dc.size(), fp) == dc.size() && fread(cp.data(), 4, cp.size(), fp) == cp.size() &&
+            fread(cw.data(), 4, cw.size(), fp) == cw.size() && fread(cd.data(), 4, cd.size(), fp) == cd.size() &&
+            fread(cr.data(), 4, cr.size(), fp) == cr.size();
+  fclose(fp);
+  if (!ok) return nnpe_fail(c, NNPE_EFILE, "weight file: truncated");
+  for (int i = 0; i < c->nbtyp; ++i) { bc[4 * i + 1] *= 2; bc[4 * i + 3] *= 2; }   // BOND::setParam()
+  for (int i = 0; i < c->natyp; ++i) { ac[4 * i + 1] *= 2; ac[4 * i + 3] *= 2; }   // ANGLE::setParam()
+  for (int i = 0; i < c->ndtyp; ++i) { dc[4 * i + 2] *= 2; dc[4 * i + 3] *= 3; }   // DIHEDRAL::setParam()
+  if (int rc = nnpe_bonded_coefs(c, bc.data(), ac.data(), dc.data())) return rc;
+  return nnpe_nnp_set(c, kind, cutoff, nbin, scale, e1, e2, h1, h2, cp.data(), cw.data(), cd.data(), cr.data(),
+                      kind ? embw.data() : nullptr, fitw.data());
+}

@@ -116,6 +116,9 @@ class Engine:
     def load_pair_table(self, nbin: int, path: str):
         self._ok(self.lib.nnpe_pair_load_table(self.h, nbin, path.encode()))
 
+    def pair_exact(self, on: bool):
+        self._ok(self.lib.nnpe_pair_exact(self.h, int(on)))
+
     def pair_enable(self, on: bool):
         self._ok(self.lib.nnpe_pair_enable(self.h, int(on)))
 
@@ -127,6 +130,37 @@ class Engine:
         dc = _f32(np.reshape(dcoef, (-1, 4))) if len(dcoef) else np.zeros((1, 4), np.float32)
         self._ok(self.lib.nnpe_bonded_set(self.h, len(b), _i32(b).ravel(), len(bc), bc.ravel(), len(a), _i32(a).ravel(),
                                           len(ac), ac.ravel(), len(d), _i32(d).ravel(), len(dc), dc.ravel()))
+
+    # ---- NNPOTENTIAL_TBL / network term ---------------------------------------------------
+    def nnp_set(self, m, cutoff=6.0, nbin=750):
+        """Install a network term (nnp_model.NnpModel) sharing the pair list."""
+        kind = 1 if m.kind == "embed" else 0
+        keep = []
+
+        def ptr(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, np.float32)
+            keep.append(a)
+            return a.ctypes.data
+
+        self._ok(self.lib.nnpe_nnp_set(self.h, kind, cutoff, nbin, m.scale, m.e1, m.e2, m.h1, m.h2, ptr(m.coef_p),
+                                       ptr(m.coef_w), ptr(m.coef_d), ptr(m.coef_r), ptr(m.embw), ptr(m.fitw)))
+
+    def nnp_load(self, cutoff: float, nbin: int, paramfile: str, wtfile: str):
+        self._ok(self.lib.nnpe_nnp_load(self.h, cutoff, nbin, paramfile.encode(), wtfile.encode()))
+
+    def nnp_precision(self, bf16: bool):
+        self._ok(self.lib.nnpe_nnp_precision(self.h, int(bf16)))
+
+    def nnp_get(self):
+        din, kind = C.c_int(0), C.c_int(0)
+        self._ok(self.lib.nnpe_nnp_info(self.h, C.byref(din), C.byref(kind)))
+        G = np.zeros(self.natom * din.value, np.float32)
+        dG = np.zeros(self.natom * din.value, np.float32)
+        e = np.zeros(self.natom)
+        self._ok(self.lib.nnpe_nnp_get(self.h, G.ctypes.data, dG.ctypes.data, e.ctypes.data))
+        return G.reshape(self.natom, -1), dG.reshape(self.natom, -1), e
 
     # ---- VERLET / thermostat ---------------------------------------------------------------
     def verlet(self, dt=1.0, fp64=True):

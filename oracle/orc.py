@@ -51,7 +51,7 @@ def _lib(prec: str) -> C.CDLL:
     lib.orc_gr_counts.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_double, _i64p, C.POINTER(C.c_int)]
     lib.orc_nnp_tbl.argtypes = [C.c_void_p, C.c_double, C.c_int, _f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, _f32p,
                                 _f64p, _f64p, _f64p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
-    lib.orc_nnp_emb.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, _f32p, C.c_int, C.c_int, _f32p,
+    lib.orc_nnp_emb.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int, _f32p, C.c_int, C.c_int, _f32p,
                                 _f64p, _f64p, _f64p, _f64p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.orc_nnp_tables.argtypes = [C.c_int, C.c_double, C.c_int, _f32p, _f32p, _f32p, _f32p, real, real, real, real]
     lib.orc_sq.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p]
@@ -135,12 +135,12 @@ class Restated:
                              _f32(coef_r).ravel(), h1, h2, _f32(fitw).ravel(), G, dG, f, C.byref(ep), C.byref(en), C.byref(w))
         return dict(G=G.reshape(n, 20), dEdG=dG.reshape(n, 20), f=f.reshape(n, 3), e_pair=ep.value, e_net=en.value, vir=w.value)
 
-    def nnp_emb(self, cutoff, e1, e2, embw, h1, h2, fitw):
+    def nnp_emb(self, cutoff, scale, e1, e2, embw, h1, h2, fitw):
         n = self.sysm.natom
         din = 4 * e2
         G = np.zeros(n * din); dG = np.zeros(n * din); ea = np.zeros(n); f = np.zeros(n * 3)
         en, w = C.c_double(0), C.c_double(0)
-        self.lib.orc_nnp_emb(self.h, cutoff, e1, e2, _f32(embw).ravel(), h1, h2, _f32(fitw).ravel(), G, dG, ea, f,
+        self.lib.orc_nnp_emb(self.h, cutoff, scale, e1, e2, _f32(embw).ravel(), h1, h2, _f32(fitw).ravel(), G, dG, ea, f,
                              C.byref(en), C.byref(w))
         return dict(G=G.reshape(n, din), dEdG=dG.reshape(n, din), e_atom=ea, f=f.reshape(n, 3), e_net=en.value, vir=w.value)
 

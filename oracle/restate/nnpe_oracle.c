@@ -634,22 +634,24 @@ int orc_nnp_tbl(const orc_t* o, double cutoff_d, int nbin, const float* coef_p, 
 }
 
 /* Radial-embedding NNP (the network of the 96k-atom workload; no counterpart in the reference's
- * C++, whose network sits behind TF): per pair type an embedding u=r/rc -> e1 (tanh) -> e2
- * (tanh) times the reference's cutoff factor cff(r) (pair_nnp.cpp:573-584), accumulated into
- * descriptor slot s*e2+c by special class s (the reference indexes its descriptor functions by
- * special class the same way, pair_nnp.cpp:663); per-species fitting network on 4*e2 inputs;
- * forces by the reference's back-projection fpair = -sum_c (dE/dG_i + dE/dG_j) d(phi_c)/dr / r
- * (pair_nnp.cpp:753-764). Embedding block per pair type: W1[e1] b1[e1] W2[e1][e2] b2[e2]. */
-int orc_nnp_emb(const orc_t* o, double cutoff_d, int e1, int e2, const float* embw, int h1, int h2,
+ * C++, whose network sits behind TF). Per neighbour species t_j an embedding net
+ * u=r/rc -> e1 (tanh) -> e2 (tanh); the pair's contribution scale*y_c(r)*cff(r), with the
+ * reference's cutoff factor cff = 1-1/(1+(r-rc)^2) (pair_nnp.cpp:573-584), is accumulated into
+ * descriptor slot s*e2+c of atom i by special class s (the reference selects its descriptor
+ * functions by special class the same way, pair_nnp.cpp:663); a per-species fitting network on
+ * the 4*e2 inputs gives E_i; forces follow the reference's back-projection
+ * fpair = -sum_c (dE/dG_i + dE/dG_j)[s*e2+c] d(phi_c)/dr / r (pair_nnp.cpp:753-764).
+ * Embedding block per species: W1[e1] b1[e1] W2[e1][e2] b2[e2]. */
+int orc_nnp_emb(const orc_t* o, double cutoff_d, double scale_d, int e1, int e2, const float* embw, int h1, int h2,
                 const float* fitw, double* G_out, double* dEdG_out, double* e_atom, double* f_by_id,
                 double* e_net, double* vir) {
   const int N = o->natom, din = 4 * e2;
-  const real rc = (real)cutoff_d, cutsq = rc * rc, r_rc = 1 / rc;
+  const real rc = (real)cutoff_d, cutsq = rc * rc, r_rc = 1 / rc, scale = (real)scale_d;
   const size_t eb = (size_t)e1 + e1 + (size_t)e1 * e2 + e2;
   real* G = (real*)calloc((size_t)N * din, sizeof(real));
   real* dG = (real*)calloc((size_t)N * din, sizeof(real));
   real* h = (real*)malloc(sizeof(real) * (e1 + e2 + e1));
-  real *y = h + e1, *t = y + e2;
+  real *t = h + e1 + e2;
   for (int i = 0; i < N; ++i) {
     const int ia = o->order[i];
     const real* xi = o->xs + 3 * i;
@@ -659,14 +661,14 @@ int orc_nnp_emb(const orc_t* o, double cutoff_d, int e1, int e2, const float* em
       real rsq = sqr(xi[0] - xj[0]) + sqr(xi[1] - xj[1]) + sqr(xi[2] - xj[2]);
       if (!(rsq < cutsq)) continue;
       real r = sqrt(rsq), u = r * r_rc;
-      int p = o->pairtype[o->typ[ia] * o->ntype + o->typ[ja]], s = special_of(o, ia, ja);
-      const float *W1 = embw + eb * p, *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
+      int s = special_of(o, ia, ja);
+      const float *W1 = embw + eb * o->typ[ja], *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
       real cf = r - rc, cff = 1 - 1 / (1 + cf * cf);
       for (int a = 0; a < e1; ++a) h[a] = tanh((real)W1[a] * u + (real)b1[a]);
       for (int c = 0; c < e2; ++c) {
         real z = (real)b2[c];
         for (int a = 0; a < e1; ++a) z += h[a] * (real)W2[(size_t)a * e2 + c];
-        G[(size_t)ia * din + s * e2 + c] += tanh(z) * cff;
+        G[(size_t)ia * din + s * e2 + c] += scale * tanh(z) * cff;
       }
     }
   }
@@ -689,8 +691,8 @@ int orc_nnp_emb(const orc_t* o, double cutoff_d, int e1, int e2, const float* em
       real rsq = sqr(dx) + sqr(dy) + sqr(dz);
       if (!(rsq < cutsq)) continue;
       real r = sqrt(rsq), u = r * r_rc;
-      int p = o->pairtype[o->typ[ia] * o->ntype + o->typ[ja]], s = special_of(o, ia, ja);
-      const float *W1 = embw + eb * p, *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
+      int s = special_of(o, ia, ja);
+      const float *W1 = embw + eb * o->typ[ja], *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
       real cf = r - rc, den = 1 + cf * cf, cff = 1 - 1 / den, dcff = 2 * cf / (den * den);
       for (int a = 0; a < e1; ++a) h[a] = tanh((real)W1[a] * u + (real)b1[a]);
       real dEdr = 0;
@@ -699,7 +701,7 @@ int orc_nnp_emb(const orc_t* o, double cutoff_d, int e1, int e2, const float* em
         real z = (real)b2[c];
         for (int a = 0; a < e1; ++a) z += h[a] * (real)W2[(size_t)a * e2 + c];
         real yc = tanh(z);
-        real ac = dG[(size_t)ia * din + s * e2 + c] + dG[(size_t)ja * din + s * e2 + c];
+        real ac = scale * (dG[(size_t)ia * din + s * e2 + c] + dG[(size_t)ja * din + s * e2 + c]);
         dEdr += ac * yc * dcff;
         real gc = ac * cff * (1 - yc * yc);
         for (int a = 0; a < e1; ++a) t[a] += gc * (real)W2[(size_t)a * e2 + c];

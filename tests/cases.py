@@ -72,3 +72,26 @@ def list_keys(rec: np.ndarray, natom: int):
 def rel_rms(a, b):
     a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+def water_bonded_raw():
+    """Raw (pre-setParam) bond/angle/dihedral coefficients of the water model, as the reference's
+    NNP weight file stores them (pair_nnp.cpp:507-512): setParam() doubles entries 1 and 3."""
+    from nnpengine_b200 import engine as E
+    a = E.angle_coef(109.47, 0, 0, WATER_ANGLE_KC)
+    return (np.array([[1.0, 0, 0, WATER_BOND_K]], np.float32), np.array([[a[0], 0, 0, WATER_ANGLE_KC]], np.float32),
+            np.zeros((1, 4), np.float32))
+
+
+def write_nnp_inputs(m, d):
+    """Model file, paramfile and reference-layout weight file of a network model into d."""
+    from nnpengine_b200 import nnp_model as NM
+    os.makedirs(d, exist_ok=True)
+    model = os.path.join(d, "model.nnpe")
+    param = os.path.join(d, "nnp.param")
+    wt = os.path.join(d, "nnp.wt")
+    NM.write_model(model, m)
+    NM.write_paramfile(param, model, 3, m.din)
+    b, a, dd = water_bonded_raw()
+    NM.write_weight_file(wt, m, b, a, dd)
+    return dict(model=model, param=param, wt=wt)

@@ -8,6 +8,10 @@ is run on the seeded cases of tests/cases.py; its outputs are stored compactly:
                  force evaluation (pair + bond + angle); cell-based and list-based g(r) counts; a
                  20-step NVE trajectory in the reference's float arithmetic (final x, v and the
                  per-step energies).
+* nnp_gauss648.npz  the same box under the reference's tabulated NNP (NNPOTENTIAL_TBL, 6 A, 750
+                 bins, 20 Gaussians per pair type and special class, pair part from coef_p) with a
+                 20->32->32->1 fitting network evaluated by the TF C-API shim: descriptor, dE/dG,
+                 network energy, forces (bonded + NNP).
 * mixture2000.npz  2000-atom two-species LJ+Coulomb liquid at 0.035 A^-3: g(r) counts to 15 A in
                  0.01 A bins, the reference's float g(r) and S(q) on 512 q points, forces.
 
@@ -70,7 +74,26 @@ def mixture2000(work):
     print("mixture2000:", s.natom, "atoms, gr bins", out["gr_counts"].shape)
 
 
+def nnp_gauss648(work):
+    from nnpengine_b200 import nnp_model as NM
+    s, table = cases.water_case()
+    f = cases.write_inputs(s, table, work)
+    v0 = os.path.join(work, "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    m = NM.gauss_model()
+    paths = cases.write_nnp_inputs(m, work)
+    snap = orc.run_ref_dump({"init": f["init"], "no_lj": "", "nnp": f"6.0 750 {paths['param']} {paths['wt']}",
+                             "skin": 2, "gr_cutoff": 6, "bond": ["1.0 0"], "angle": ["109.47 0 0 0"],
+                             "velocity": v0, "mode": "snapshot"}, os.path.join(work, "snap"))
+    out = dict(x=s.x, desc=snap["desc"].reshape(s.natom, 20), dedg=snap["dedg"].reshape(s.natom, 20),
+               force=snap["force"].reshape(-1, 3), f_bonded=snap["f_classical"].reshape(-1, 3),
+               erg_f32=snap["log_e"], enn=snap["log_enn"])
+    np.savez_compressed(os.path.join(HERE, "nnp_gauss648.npz"), **out)
+    print("nnp_gauss648: network energy", float(snap["log_enn"][0]))
+
+
 if __name__ == "__main__":
     with tempfile.TemporaryDirectory() as t:
         water648(os.path.join(t, "w"))
         mixture2000(os.path.join(t, "m"))
+        nnp_gauss648(os.path.join(t, "n"))

@@ -1,0 +1,87 @@
+"""Network term on the GPU: the reference's tabulated NNP against its own C++ (golden vectors),
+the embedding network against the FP64 oracle, and the BF16 tensor-core form's stated error."""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from nnpengine_b200 import engine as E
+from nnpengine_b200 import nnp_model as NM
+from nnpengine_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def nnp_engine(s, model=None, files=None, lj_table=None, cutoff=6.0, nbin=750):
+    e = Engine(0)
+    e.set_system(s)
+    e.set_velocities(np.zeros_like(s.v))
+    if lj_table is not None:
+        e.setup(10.0, 2.0, 10.0, 2048)
+        e.set_pair_table(*lj_table)
+    else:
+        e.setup(cutoff, 2.0, cutoff, 2048)
+        e.pair_enable(False)
+    b, a, d = cases.water_bonded_raw()
+    e.set_bonded(s, [b[0] * np.array([1, 2, 1, 2], np.float32)], [a[0] * np.array([1, 2, 1, 2], np.float32)], [d[0]])
+    if files is not None:
+        e.nnp_load(cutoff, nbin, files["param"], files["wt"])
+    else:
+        e.nnp_set(model, cutoff, nbin)
+    return e
+
+
+def test_gauss_nnp_matches_reference(tmp_path):
+    g = np.load(os.path.join(cases.GOLDEN, "nnp_gauss648.npz"))
+    s, _ = cases.water_case()
+    m = NM.gauss_model()
+    files = cases.write_nnp_inputs(m, str(tmp_path))
+    e = nnp_engine(s, files=files)
+    e.list_build()
+    erg, vir = e.compute_forces(True)
+    G, dG, ea = e.nnp_get()
+    np.testing.assert_allclose(G, g["desc"], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(dG, g["dedg"], rtol=1e-4, atol=1e-6)
+    assert abs(ea.sum() - g["enn"][0]) / abs(g["enn"][0]) < 1e-5
+    assert cases.rel_rms(e.forces(), g["force"]) < 1e-5
+
+
+def test_embed_nnp_fp32_matches_fp64_oracle():
+    from oracle import orc
+    s, table = cases.water_case()
+    m = NM.embed_model()
+    e = nnp_engine(s, model=m)
+    e.list_build()
+    erg, vir = e.compute_forces(True)
+    G, dG, ea = e.nnp_get()
+    o = orc.Restated(s, "f64")
+    assert o.rebuild(s.x, 6, 2, 8) == 0
+    r = o.nnp_emb(6.0, m.scale, m.e1, m.e2, m.embw, m.h1, m.h2, m.fitw)
+    assert cases.rel_rms(G, r["G"]) < 1e-5
+    assert cases.rel_rms(dG, r["dEdG"]) < 1e-4
+    assert abs(ea.sum() - r["e_net"]) / abs(r["e_net"]) < 1e-5
+    fb, _, _ = o.bonded(*[x * np.array([1, 2, 1, 2], np.float32) for x in cases.water_bonded_raw()[:2]],
+                        np.zeros((1, 4), np.float32))
+    f = e.forces()
+    assert cases.rel_rms(f, r["f"] + fb) < 1e-5
+
+
+def test_embed_nnp_plus_lj_composed():
+    """Tabulated LJ/Coulomb at 10 A plus the network at 6 A on one 12 A list."""
+    from oracle import orc
+    s, table = cases.water_case()
+    F, U = cases.table_as_loaded(table[1], table[2])
+    m = NM.embed_model()
+    e = nnp_engine(s, model=m, lj_table=(F, U))
+    e.list_build()
+    erg, vir = e.compute_forces(True)
+    o = orc.Restated(s, "f64")
+    assert o.rebuild(s.x, 10, 2, 12) == 0
+    fp, ep, wp = o.pair_forces(F, U, 10.0)
+    r = o.nnp_emb(6.0, m.scale, m.e1, m.e2, m.embw, m.h1, m.h2, m.fitw)
+    fb, eb, wb = o.bonded(*[x * np.array([1, 2, 1, 2], np.float32) for x in cases.water_bonded_raw()[:2]],
+                          np.zeros((1, 4), np.float32))
+    ref = fp + r["f"] + fb
+    assert cases.rel_rms(e.forces(), ref) < 1e-5
+    assert abs(erg - (ep + r["e_net"] + eb)) / abs(ep + r["e_net"] + eb) < 1e-5

@@ -96,3 +96,21 @@ def test_reference_harness_reproducible(tmp_path):
                           "velocity": v0, "mode": "snapshot"}, str(tmp_path / "o"))
     np.testing.assert_array_equal(r["force"].reshape(-1, 3), g["force"])
     np.testing.assert_array_equal(r["gr_counts"].reshape(3, -1), g["gr_counts"])
+
+
+def test_restated_nnp_tbl_matches_reference():
+    """The restated NNPOTENTIAL_TBL (tables, descriptor, fitting net, back-projection) against the
+    reference's own C++ with the shim network."""
+    from nnpengine_b200 import nnp_model as NM
+    g = np.load(os.path.join(cases.GOLDEN, "nnp_gauss648.npz"))
+    s, _ = cases.water_case()
+    m = NM.gauss_model()
+    o = orc.Restated(s, "f32")
+    assert o.rebuild(s.x, 6, 2, 8) == 0
+    r = o.nnp_tbl(6.0, 750, m.coef_p, m.coef_w, m.coef_d, m.coef_r, m.h1, m.h2, m.fitw)
+    np.testing.assert_allclose(r["G"], g["desc"], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(r["dEdG"], g["dedg"], rtol=1e-4, atol=1e-6)
+    assert abs(r["e_net"] - g["enn"][0]) / abs(g["enn"][0]) < 1e-6
+    fb, _, _ = o.bonded(*[np.asarray(x) * np.array([1, 2, 1, 2], np.float32) for x in cases.water_bonded_raw()[:2]],
+                        np.zeros((1, 4), np.float32))
+    assert cases.rel_rms(r["f"] + fb, g["force"]) < 1e-5

@@ -18,7 +18,7 @@ FORCE_RTOL = 1e-5
 ENERGY_RTOL = 1e-6
 
 
-def water_engine(fp64=False, cap=2048, v=None):
+def water_engine(fp64=False, cap=2048, v=None, exact=False):
     s, table = cases.water_case()
     F, U = cases.table_as_loaded(table[1], table[2])
     e = Engine(0)
@@ -29,6 +29,7 @@ def water_engine(fp64=False, cap=2048, v=None):
     e.set_pair_table(F, U)
     e.set_bonded(s, [E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)], [E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)])
     e.verlet(1.0, fp64)
+    e.pair_exact(exact)
     return s, (F, U), e
 
 
@@ -57,9 +58,10 @@ def test_neighbour_list_bit_exact():
     np.testing.assert_array_equal(digests, g["list_digests"])
 
 
-def test_forces_and_energy():
+@pytest.mark.parametrize("exact", [True, False])
+def test_forces_and_energy(exact):
     g = golden("water648.npz")
-    s, (F, U), e = water_engine()
+    s, (F, U), e = water_engine(exact=exact)
     e.list_build()
     erg, vir = e.compute_forces(ev=True)
     f = e.forces()
@@ -122,7 +124,7 @@ def test_mixture_gr_counts_and_sq():
 
 def test_nve_trajectory_fp32_matches_reference():
     g = golden("water648.npz")
-    s, _, e = water_engine(fp64=False)
+    s, _, e = water_engine(fp64=False, exact=True)
     log = e.run(21, log_interval=1)
     assert len(log) == 21
     x, v = e.positions(), e.velocities()
