@@ -188,6 +188,10 @@ int nnpe_nnp_precision(nnpe_ctx* ctx, int bf16);
 int nnpe_nnp_get(nnpe_ctx* ctx, float* G, float* dEdG, double* e_atom);
 int nnpe_nnp_info(nnpe_ctx* ctx, int* din, int* kind);
 
+/* Self-test of the tcgen05 tile path on `device`: D[128][N] = bf16(A[128][K]) x bf16(B[N][K])^T,
+ * FP32 accumulation in tensor memory (16 <= N <= 256, 16 <= K <= 128, multiples of 16). */
+int nnpe_tc_selftest(int device, int N, int K, const float* A, const float* B, float* D);
+
 /* ---- profiling ------------------------------------------------------------------------
  * Enqueue one kernel class without synchronising (for event timing): 0 pair force, 1 list
  * rebuild, 2 bonded, 3 network term, 4 Verlet, 5 cell-based g(r), 6 list-based g(r). */

@@ -47,7 +47,7 @@ def _compile(unit: str, flags, verbose: bool) -> str:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OUT, exist_ok=True)
-    srcs = [os.path.join(CSRC, u) for u in UNITS] + [os.path.join(CSRC, "internal.cuh"), os.path.join(CSRC, "nnp.cuh"),
+    srcs = [os.path.join(CSRC, u) for u in UNITS] + [os.path.join(CSRC, "internal.cuh"), os.path.join(CSRC, "nnp.cuh"), os.path.join(CSRC, "tc_util.cuh"),
                                                      os.path.join(HERE, "..", "include", "nnpe.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) > max(os.path.getmtime(s) for s in srcs):
         return LIB

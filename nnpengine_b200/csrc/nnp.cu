@@ -100,6 +100,8 @@ static void gen_tables(int npair, float cutoff, int nbin, const float* coef_p_in
 }
 
 static size_t fit_block(int din, int h1, int h2) { return (size_t)din * h1 + h1 + (size_t)h1 * h2 + h2 + h2 + 1; }
+static constexpr int kEmbWarpsHost = 4;
+static int nnp_set_smem_attrs(nnpe_ctx* c, int smem_desc, int smem_force);
 
 int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, int e1, int e2, int h1, int h2,
                  const float* coef_p, const float* coef_w, const float* coef_d, const float* coef_r, const float* embw,
@@ -149,6 +151,12 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   std::vector<int> cnt(c->ntype, 0);
   for (int t : c->h_typ) ++cnt[t];
   for (int t = 0; t < c->ntype; ++t) m->soff[t + 1] = m->soff[t] + cnt[t];
+  if (kind == 1) {
+    const size_t eb = (size_t)32 + 32 + 32 * (size_t)e2 + e2;
+    const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * 32 * (e2 + 1)) + sizeof(int) * kEmbWarpsHost * 32);
+    const int smem_force = (int)(sizeof(float) * eb * c->ntype);
+    if (int r2 = nnp_set_smem_attrs(c, smem_desc, smem_force)) return r2;
+  }
   c->graph_valid = false;
   return nnp_tc_setup(c);
 }
@@ -550,6 +558,14 @@ __global__ void __launch_bounds__(256) k_fit_gemm(FitArgs f) {
 }
 
 }  // namespace
+
+static int nnp_set_smem_attrs(nnpe_ctx* c, int smem_desc, int smem_force) {
+  static_assert(kEmbWarps == kEmbWarpsHost, "warp count");
+  NNPE_CUDA(c, cudaFuncSetAttribute(k_emb_desc_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_desc));
+  NNPE_CUDA(c, cudaFuncSetAttribute(k_emb_force_f32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
+  NNPE_CUDA(c, cudaFuncSetAttribute(k_emb_force_f32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
+  return 0;
+}
 
 static NnpArgs make_args(nnpe_ctx* c) {
   NnpModel* m = c->nnp;

@@ -21,8 +21,13 @@ WATER_BOND_K = 450.0
 WATER_ANGLE_KC = 62.0
 
 
-def water_case(n_side=6, bl=18.624, seed=1, temperature=300.0, nmol=None):
+def water_case(n_side=6, bl=18.624, seed=1, temperature=300.0, nmol=None, jitter=0.0):
+    """jitter > 0 displaces atoms by seeded N(0, jitter) so that bonds and angles are off their
+    equilibrium (the lattice start sits exactly on it, where FP32 bonded forces are rounding noise)."""
     s = S.water_box(n_side, bl, seed=seed, temperature=temperature, nmol=nmol)
+    if jitter > 0:
+        rng = np.random.default_rng(seed + 1000)
+        s.x = (s.x + rng.normal(0, jitter, s.x.shape)).astype(np.float32)
     r, F, U = S.water_lj_table(10.0, 1000)
     return s, (r, F, U)
 

@@ -49,7 +49,7 @@ def test_gauss_nnp_matches_reference(tmp_path):
 
 def test_embed_nnp_fp32_matches_fp64_oracle():
     from oracle import orc
-    s, table = cases.water_case()
+    s, table = cases.water_case(jitter=0.05)
     m = NM.embed_model()
     e = nnp_engine(s, model=m)
     e.list_build()
@@ -70,7 +70,7 @@ def test_embed_nnp_fp32_matches_fp64_oracle():
 def test_embed_nnp_plus_lj_composed():
     """Tabulated LJ/Coulomb at 10 A plus the network at 6 A on one 12 A list."""
     from oracle import orc
-    s, table = cases.water_case()
+    s, table = cases.water_case(jitter=0.05)
     F, U = cases.table_as_loaded(table[1], table[2])
     m = NM.embed_model()
     e = nnp_engine(s, model=m, lj_table=(F, U))
@@ -85,3 +85,66 @@ def test_embed_nnp_plus_lj_composed():
     ref = fp + r["f"] + fb
     assert cases.rel_rms(e.forces(), ref) < 1e-5
     assert abs(erg - (ep + r["e_net"] + eb)) / abs(ep + r["e_net"] + eb) < 1e-5
+
+
+def _bf16_vs_fp64(s, m, e):
+    from oracle import orc
+    o = orc.Restated(s, "f64")
+    assert o.rebuild(s.x, 6, 2, 8) == 0
+    r = o.nnp_emb(6.0, m.scale, m.e1, m.e2, m.embw, m.h1, m.h2, m.fitw)
+    G, dG, ea = e.nnp_get()
+    return r, G, dG, ea
+
+
+def test_embed_nnp_bf16_tensor_core_error_vs_fp64():
+    """BF16 operands on tcgen05 (FP32 accumulate): network force RMSE within 1% of the force RMS
+    against the FP64 oracle (the stated bar), descriptor and energy errors reported the same way."""
+    s, _ = cases.water_case(jitter=0.05)
+    m = NM.embed_model()
+    e = nnp_engine(s, model=m)
+    e.pair_enable(False)
+    e.set_bonded(s, [], [], [])
+    e.nnp_precision(True)
+    e.list_build()
+    erg, vir = e.compute_forces(True)
+    assert e.device_errors() == 0
+    r, G, dG, ea = _bf16_vs_fp64(s, m, e)
+    f = e.forces()
+    err_G = cases.rel_rms(G, r["G"])
+    err_dG = cases.rel_rms(dG, r["dEdG"])
+    err_f = cases.rel_rms(f, r["f"])
+    err_e = abs(ea.sum() - r["e_net"]) / abs(r["e_net"])
+    print(f"BF16 vs FP64: G {err_G:.2e} dE/dG {err_dG:.2e} force {err_f:.2e} energy {err_e:.2e}")
+    assert err_G < 1e-2
+    assert err_dG < 3e-2
+    assert err_f < 1e-2
+    assert err_e < 1e-2
+
+
+def test_embed_nnp_bf16_deterministic():
+    s, _ = cases.water_case(jitter=0.05)
+    m = NM.embed_model()
+    e = nnp_engine(s, model=m)
+    e.nnp_precision(True)
+    e.list_build()
+    e.compute_forces(True)
+    f1 = e.forces().copy()
+    e.compute_forces(True)
+    np.testing.assert_array_equal(e.forces(), f1)
+
+
+def test_embed_nnp_bf16_md_steps():
+    """A few MD steps on the tensor-core path: finite, no device errors, graph replay matches."""
+    s, table = cases.water_case(jitter=0.05)
+    F, U = cases.table_as_loaded(table[1], table[2])
+    m = NM.embed_model()
+    logs = []
+    for graph in (False, True):
+        e = nnp_engine(s, model=m, lj_table=(F, U))
+        e.set_velocities(s.v)
+        e.nnp_precision(True)
+        e.verlet(0.5, True)
+        logs.append((e.run(20, log_interval=5, graph=graph), e.positions(f64=True)))
+        assert e.device_errors() == 0
+    assert all(np.isfinite(r["erg"]) for r in logs[0][0])
+    np.testing.assert_array_equal(logs[0][1], logs[1][1])
