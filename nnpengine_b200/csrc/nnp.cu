@@ -151,6 +151,8 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   std::vector<int> cnt(c->ntype, 0);
   for (int t : c->h_typ) ++cnt[t];
   for (int t = 0; t < c->ntype; ++t) m->soff[t + 1] = m->soff[t] + cnt[t];
+  if ((rc = nalloc(c, &m->d_soff_dev, NNPE_MAX_TYPES + 1))) return rc;
+  NNPE_CUDA(c, cudaMemcpy(m->d_soff_dev, m->soff.data(), sizeof(int) * m->soff.size(), cudaMemcpyHostToDevice));
   if (kind == 1) {
     const size_t eb = (size_t)32 + 32 + 32 * (size_t)e2 + e2;
     const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * 32 * (e2 + 1)) + sizeof(int) * kEmbWarpsHost * 32);
@@ -614,8 +616,6 @@ static int fit_f32_enqueue(nnpe_ctx* c) {
 
 int nnp_species_enqueue(nnpe_ctx* c) {
   NnpModel* m = c->nnp;
-  if (!m->d_soff_dev) NNPE_CUDA(c, cudaMalloc(&m->d_soff_dev, sizeof(int) * (NNPE_MAX_TYPES + 1)));
-  NNPE_CUDA(c, cudaMemcpyAsync(m->d_soff_dev, m->soff.data(), sizeof(int) * m->soff.size(), cudaMemcpyHostToDevice, c->stream));
   NNPE_CUDA(c, cudaMemsetAsync(m->d_scount, 0, sizeof(int) * NNPE_MAX_TYPES, c->stream));
   k_species<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_info, m->d_sidx, m->d_scount, m->d_soff_dev, c->natom);
   NNPE_CHECK_LAUNCH(c);
