@@ -29,11 +29,30 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 WORKLOADS = {
-    # name: (n_side, bl, nmol, description)
+    "water96k-nnp-bf16": dict(n_side=32, bl=99.3, nmol=32000, nnp="bf16",
+                              desc="96,000-atom water (32,000 molecules, 99.3 A box): tabulated LJ + DSF Coulomb at 10 A "
+                                   "plus the radial-embedding network at 6 A (1->32->64 per species, 4 special-class "
+                                   "slots, fitting 256->128->128->1, tanh) with BF16 tcgen05 GEMMs and FP32 accumulation; "
+                                   "2 A skin, bonds + angles, dt 0.5 fs NVE, FP64 Verlet state"),
+    "water96k-nnp-fp32": dict(n_side=32, bl=99.3, nmol=32000, nnp="fp32",
+                              desc="the same 96,000-atom NNP + tabulated workload with the network in FP32 on CUDA cores "
+                                   "(the plain form)"),
     "water96k-classical": dict(n_side=32, bl=99.3, nmol=32000, nnp=None,
                                desc="96,000-atom water (32,000 molecules, 99.3 A box), tabulated LJ + DSF Coulomb at "
                                     "10 A, 2 A skin, bonds + angles, dt 0.5 fs NVE, FP64 Verlet state"),
+    "water3k-classical": dict(n_side=10, bl=31.04, nmol=None, nnp=None,
+                              desc="3,000-atom water (1,000 molecules, 31.04 A box), tabulated LJ + DSF Coulomb at 10 A, "
+                                   "2 A skin, bonds + angles, dt 0.5 fs NVE"),
 }
+
+
+def nnp_flops_per_step(natom, pairs6):
+    """Algorithmic network FLOPs of one force evaluation: per pair the embedding's two layers
+    forward and their input-gradient backward (2*(32 + 32*64) MAC each way), per atom the fitting
+    network forward (256*128 + 128*128 + 128 MAC) and backward (128*128 + 128*256 MAC)."""
+    per_pair = 2 * 2 * (32 + 32 * 64)
+    per_atom = 2 * (256 * 128 + 128 * 128 + 128) + 2 * (128 * 128 + 128 * 256)
+    return pairs6 * per_pair + natom * per_atom
 
 
 def peaks():
@@ -99,38 +118,65 @@ class ClockSampler:
 def build_system(wl):
     import cases
     from nnpengine_b200 import systems as S
-    s = S.water_box(wl["n_side"], wl["bl"], seed=2, nmol=wl["nmol"])
+    s = S.water_box(wl["n_side"], wl["bl"], seed=2, nmol=wl.get("nmol"))
     r, F, U = S.water_lj_table(10.0, 1000)
     return s, (r, F, U)
 
 
-def make_engine(s, table, device):
+def make_engine(s, table, device, nnp=None):
     import cases
     from nnpengine_b200 import engine as E
+    from nnpengine_b200 import nnp_model as NM
     F, U = cases.table_as_loaded(table[1], table[2])
     e = E.Engine(device)
     e.set_system(s)
     e.setup(10.0, 2.0, 10.0, 1024)
     e.set_pair_table(F, U)
     e.set_bonded(s, [E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)], [E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)])
+    if nnp:
+        e.nnp_set(NM.embed_model(), 6.0, 750)
+        e.nnp_precision(nnp == "bf16")
     return e
 
 
 def cpu_reference(wl, steps: int):
-    """The reference's OpenMP force step (oracle/_ref/ref_dump_fast) on the same workload, timed
-    over its MD loop only; returns (atom-steps/s, threads, sample description)."""
+    """The reference's own OpenMP force step on the same system (oracle/_ref/ref_dump_fast): its
+    LJTableCoulDSF + bonded terms, and for network workloads its tabulated NNP (NNPOTENTIAL_TBL at
+    6 A with a 20->128->128->1 fitting network behind the TF C-API shim; the reference cannot run
+    the embedding network). Timed over its MD loop only; returns (atom-steps/s, threads, sample)."""
     from oracle import orc
     import cases
+    from nnpengine_b200 import nnp_model as NM
     s, table = build_system(wl)
     with tempfile.TemporaryDirectory() as d:
         f = cases.write_inputs(s, table, d)
         cfg = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10,
                "bond": [f"1.0 {cases.WATER_BOND_K}"], "angle": [f"109.47 0 0 {cases.WATER_ANGLE_KC}"],
                "velocity": f["vel"], "mode": "md", "steps": steps, "dt": 0.5, "log_interval": steps}
+        what = "LJ/DSF table + bonded"
+        if wl.get("nnp"):
+            paths = cases.write_nnp_inputs(NM.gauss_model(h1=128, h2=128), d)
+            cfg["nnp"] = f"6.0 750 {paths['param']} {paths['wt']}"
+            what += " + its tabulated NNP (20 Gaussians/slot, 20->128->128->1 net via the C-API shim)"
         out = orc.run_ref_dump(cfg, os.path.join(d, "o"), fast=True, timeout=1800)
     t = float(out["info"]["t_loop"])
     n = steps + 1   # md_step = 0..steps inclusive
-    return s.natom * n / t, int(out["info"]["threads"]), f"{n} MD steps of the {s.natom}-atom workload, MD loop only"
+    ncpu = os.cpu_count()
+    return (s.natom * n / t, int(out["info"]["threads"]),
+            f"{n} MD steps of the {s.natom}-atom system ({what}), MD loop only, {out['info']['threads']} OpenMP "
+            f"threads on a {ncpu}-CPU host")
+
+
+def time_enqueue(e, stream, which, reps):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e._ok(e.lib.nnpe_profile_enqueue(e.h, which))
+    a.record(stream)
+    for _ in range(reps):
+        e._ok(e.lib.nnpe_profile_enqueue(e.h, which))
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
 
 
 def main():
@@ -139,11 +185,13 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="water96k-classical", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="water96k-nnp-bf16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the plain FP32 network alongside")
     ap.add_argument("--exact", action="store_true", help="pair forces in the reference's exact float sequence")
-    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--equil", type=int, default=5000)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -173,16 +221,23 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
 
     s, table = build_system(wl)
-    e = make_engine(s, table, local)
+    e = make_engine(s, table, local, wl.get("nnp"))
     e.pair_exact(args.exact)
     stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
-    # untimed equilibration from the lattice start (Andersen, 300 K), then NVE at dt=0.5 fs
+    # untimed equilibration of the classical model from the lattice start (Andersen at 300 K,
+    # dt 1 fs, the 5 ps of the workload's definition), then the network on and NVE at dt=0.5 fs
     e.verlet(1.0, True)
     e.thermostat("andersen", 300.0, 300.0, interval=1, frac=0.1, seed=11, total_steps=0)
-    e.run(300, log_interval=300, graph=True)
+    if wl.get("nnp"):
+        e.nnp_enable(False)
+    if args.equil:
+        e.run(args.equil, log_interval=args.equil, graph=True)
+    if wl.get("nnp"):
+        e.nnp_enable(True)
     e.thermostat("none")
     e.verlet(0.5, True)
-    e.run(args.warmup, log_interval=max(args.warmup, 1), graph=True)
+    wlog = e.run(args.warmup, log_interval=max(args.warmup, 1), graph=True)
+    nbuild0 = wlog[-1]["nbuild"] if wlog else 0
 
     torch.cuda.synchronize()
     if dist:
@@ -203,46 +258,75 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     info = e.list_info()
+    nbuild_timed = (log[-1]["nbuild"] if log else info["nbuild"]) - nbuild0
     value = s.natom * args.steps * world / (ms / 1e3)
+    launches = int(e.lib.nnpe_launches_per_step(e.h))
 
-    # dominant kernel: the pair force, timed alone with CUDA events on the library stream
-    nlist = info["entries"] / s.natom
-    reps = 50
-    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # per-kernel-class device time (CUDA events on the library stream)
+    reps = 20
     e.compute_forces(ev=False)
-    k0.record(stream)
-    for _ in range(reps):
-        e.lib.nnpe_profile_enqueue(e.h, 0)
-    k1.record(stream)
-    torch.cuda.synchronize()
-    pair_ms = k0.elapsed_time(k1) / reps
+    kms = {"pair": time_enqueue(e, stream, 0, reps), "bonded": time_enqueue(e, stream, 2, reps),
+           "verlet": time_enqueue(e, stream, 4, reps), "rebuild": time_enqueue(e, stream, 1, 5)}
+    if wl.get("nnp"):
+        kms["network"] = time_enqueue(e, stream, 3, reps)
     hbm, bf16, bf16s, src = peaks()
-    alg_bytes = s.natom * (4 * nlist + 48)
-    achieved = alg_bytes / (pair_ms / 1e3) / 1e9
+    nlist = info["entries"] / s.natom
+    if wl.get("nnp"):
+        # network pairs inside 6 A from the compact list of the last evaluation
+        G, dG, ea = e.nnp_get()
+        pairs6 = int(e.lib.nnpe_nnp_pairs(e.h))
+        flops = nnp_flops_per_step(s.natom, pairs6)
+        ach = flops / (kms["network"] / 1e3) / 1e12
+        roof = {"bound": "tensor", "kernel": "network (k_tc_desc + k_tc_fit + k_tc_force)" if wl["nnp"] == "bf16"
+                else "network (FP32 CUDA cores)", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
+                "traffic": None, "peak_source": src, "kernel_ms": kms["network"], "alg_flops_per_launch": flops,
+                "pairs_in_6A_per_atom": pairs6 / s.natom}
+    else:
+        alg_bytes = s.natom * (4 * nlist + 48)
+        ach = alg_bytes / (kms["pair"] / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_pair", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "peak_source": src, "kernel_ms": kms["pair"], "alg_bytes_per_launch": alg_bytes}
 
-    # end to end through the public API with host buffers: positions in, forces + energy out
-    n3 = s.natom * 3
-    x_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
-    f_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
-    x0 = e.positions().astype(np.float32)
-    v0 = e.velocities().astype(np.float32)
-    import ctypes as C
-    erg = C.c_double(0)
-    e2e_steps = max(10, args.steps // 4)
-    xs = [(x0 + np.float32(k * 0.5) * v0).ravel() for k in range(e2e_steps + 3)]
-    for k in range(3):
-        x_host.numpy()[:] = xs[k]
-        e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), C.byref(erg), None))
-    torch.cuda.synchronize()
-    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    h0.record(stream)
-    for k in range(e2e_steps):
-        x_host.numpy()[:] = xs[3 + k]
-        e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), C.byref(erg), None))
-    h1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = h0.elapsed_time(h1) / e2e_steps
-    e2e_value = s.natom * world / (e2e_ms / 1e3)
+    plain = None
+    if wl.get("nnp") == "bf16" and not args.no_compare:
+        e.nnp_precision(False)
+        e.run(5, log_interval=5, graph=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nfp = max(20, args.steps // 4)
+        a.record(stream)
+        e.run(nfp, log_interval=nfp, graph=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        plain = s.natom * world / (a.elapsed_time(b) / nfp / 1e3)
+        e.nnp_precision(True)
+
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as C
+        n3 = s.natom * 3
+        x_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
+        f_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
+        x0 = e.positions().astype(np.float32)
+        v0 = e.velocities().astype(np.float32)
+        erg = C.c_double(0)
+        e2e_steps = max(10, args.steps // 4)
+        xs = [(x0 + np.float32(k * 0.5) * v0).ravel() for k in range(e2e_steps + 3)]
+        for k in range(3):
+            x_host.numpy()[:] = xs[k]
+            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), C.byref(erg), None))
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        for k in range(e2e_steps):
+            x_host.numpy()[:] = xs[3 + k]
+            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), C.byref(erg), None))
+        h1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = h0.elapsed_time(h1) / e2e_steps
+        e2e = {"value": s.natom * world / (e2e_ms / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": n3 * 4,
+               "d2h_bytes_per_step": n3 * 4 + 8, "ms_per_step": e2e_ms,
+               "call": "nnpe_force_step (positions in, forces + FP64 energy out, list check/rebuild on device)"}
 
     if rank == 0:
         cpu = None
@@ -253,22 +337,21 @@ def main():
             except Exception as ex:  # the reference harness is optional on a box without it
                 cpu = {"value": None, "unit": "atom-steps/s", "cores": 0, "kind": "reference",
                        "sample": f"unavailable: {ex}"}
+        cfg = {"workload": args.workload, "description": wl["desc"], "natom": s.natom,
+               "list_entries_per_atom": round(nlist, 1), "rebuilds_in_timed_steps": nbuild_timed,
+               "l2": "inputs larger than L2 (neighbour list %.0f MB)" % (info["entries"] * 4 / 1e6),
+               "ns_per_day": value / world / s.natom * 0.5 * 86400 * 1e-6, "kernel_ms": kms,
+               "pair_math": "exact float sequence" if args.exact else "rsqrt+FMA (same cutoff test)"}
+        if plain is not None:
+            cfg["plain_fp32_value"] = plain
+            cfg["bf16_over_fp32"] = value / plain
         out = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded water box, lattice start equilibrated 300 steps)",
-            "config": {"workload": args.workload, "description": wl["desc"], "natom": s.natom,
-                       "list_entries_per_atom": round(nlist, 1), "nbuild": info["nbuild"],
-                       "l2": "inputs larger than L2 (neighbour list %.0f MB)" % (info["entries"] * 4 / 1e6),
-                       "ns_per_day": value / world / s.natom * 0.5 * 86400 * 1e-6},
-            "roofline": {"bound": "hbm", "kernel": "k_pair", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
-                         "kernel_ms": pair_ms, "alg_bytes_per_launch": alg_bytes},
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": n3 * 4,
-                    "d2h_bytes_per_step": n3 * 4 + 8, "ms_per_step": e2e_ms},
-            "clocks": clk.summary(),
-            "gpu_launches": int(e.lib.nnpe_launches_per_step(e.h)) * args.steps,
+            "vs_baseline": None, "dtype": "bf16" if wl.get("nnp") == "bf16" else "f32",
+            "data": "synthetic (seeded water box, lattice start equilibrated %d steps)" % args.equil,
+            "config": cfg, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+            "gpu_launches": launches * args.steps,
         }
         print(json.dumps(out))
     if dist:

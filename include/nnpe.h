@@ -182,11 +182,15 @@ int nnpe_nnp_set(nnpe_ctx* ctx, int kind, double cutoff, int nbin, double scale,
  * coefficients, coef_p, coef_w, coef_d, coef_r, pair_nnp.cpp:505-519), which, as in the reference,
  * also sets the bonded coefficients. */
 int nnpe_nnp_load(nnpe_ctx* ctx, double cutoff, int nbin, const char* paramfile, const char* wtfile);
+/* Switch the network term off/on (kept loaded). */
+int nnpe_nnp_enable(nnpe_ctx* ctx, int on);
 /* 0: FP32 on CUDA cores (the plain form); 1: BF16 operands on tcgen05 tensor cores, FP32 accumulate. */
 int nnpe_nnp_precision(nnpe_ctx* ctx, int bf16);
 /* Descriptor G, dE/dG (atom-id order, [natom][din]) and per-atom network energy of the last evaluation. */
 int nnpe_nnp_get(nnpe_ctx* ctx, float* G, float* dEdG, double* e_atom);
 int nnpe_nnp_info(nnpe_ctx* ctx, int* din, int* kind);
+/* Pairs inside the network cutoff in the last evaluation (sum over atoms of the full list's count). */
+int64_t nnpe_nnp_pairs(nnpe_ctx* ctx);
 
 /* Self-test of the tcgen05 tile path on `device`: D[128][N] = bf16(A[128][K]) x bf16(B[N][K])^T,
  * FP32 accumulation in tensor memory (16 <= N <= 256, 16 <= K <= 128, multiples of 16). */

@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(1024) k_reduce(const double* eatom, const doub
 }  // namespace
 
 const double* nnp_atom_energy_ptr(nnpe_ctx* c);   // nnp.cu
+bool nnp_enabled(nnpe_ctx* c);
 
 int pair_enqueue(nnpe_ctx* c, bool ev) {
   const int N = c->natom;
@@ -403,7 +404,7 @@ int forces_enqueue(nnpe_ctx* c, bool ev) {
   } else {
     k_zero_forces<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_frc, c->d_eatom, c->d_watom, c->natom);
   }
-  if (c->nnp)
+  if (c->nnp && nnp_enabled(c))
     if (int rc = nnp_forces_enqueue(c, ev)) return rc;
   if (int rc = bonded_enqueue(c, ev)) return rc;
   NNPE_CHECK_LAUNCH(c);

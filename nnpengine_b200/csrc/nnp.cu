@@ -52,7 +52,15 @@ void nnp_free(nnpe_ctx* c) {
   c->nnp = nullptr;
 }
 
-const double* nnp_atom_energy_ptr(nnpe_ctx* c) { return c->nnp ? c->nnp->d_enet : nullptr; }
+const double* nnp_atom_energy_ptr(nnpe_ctx* c) { return c->nnp && c->nnp->enabled ? c->nnp->d_enet : nullptr; }
+bool nnp_enabled(nnpe_ctx* c) { return c->nnp && c->nnp->enabled; }
+
+int nnpe_nnp_enable(nnpe_ctx* c, int on) {
+  if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_enable: no network");
+  c->nnp->enabled = on != 0;
+  c->graph_valid = false;
+  return NNPE_OK;
+}
 
 // pair_nnp.cpp:521-590 in the reference's float arithmetic (exp is the C library's float exp).
 static void gen_tables(int npair, float cutoff, int nbin, const float* coef_p_in, const float* coef_w,
@@ -745,4 +753,16 @@ int nnpe_nnp_load(nnpe_ctx* c, double cutoff, int nbin, const char* paramfile, c
   if (int rc = nnpe_bonded_coefs(c, bc.data(), ac.data(), dc.data())) return rc;
   return nnpe_nnp_set(c, kind, cutoff, nbin, scale, e1, e2, h1, h2, cp.data(), cw.data(), cd.data(), cr.data(),
                       kind ? embw.data() : nullptr, fitw.data());
+}
+
+// Total pairs inside the network cutoff in the last evaluation (sum of the compact list counts).
+int64_t nnpe_nnp_pairs(nnpe_ctx* c) {
+  if (!c || !c->nnp) return -1;
+  std::vector<int> n(c->natom);
+  if (cudaMemcpyAsync(n.data(), c->nnp->d_n6, sizeof(int) * c->natom, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return -1;
+  int64_t s = 0;
+  for (int v : n) s += v;
+  return s;
 }

@@ -150,6 +150,9 @@ class Engine:
     def nnp_load(self, cutoff: float, nbin: int, paramfile: str, wtfile: str):
         self._ok(self.lib.nnpe_nnp_load(self.h, cutoff, nbin, paramfile.encode(), wtfile.encode()))
 
+    def nnp_enable(self, on: bool):
+        self._ok(self.lib.nnpe_nnp_enable(self.h, int(on)))
+
     def nnp_precision(self, bf16: bool):
         self._ok(self.lib.nnpe_nnp_precision(self.h, int(bf16)))
 

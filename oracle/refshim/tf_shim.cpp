@@ -134,9 +134,10 @@ void TF_SessionRun(TF_Session* session, const TF_Buffer*, const TF_Output*, TF_T
   TF_Tensor* tD = TF_AllocateTensor(TF_FLOAT, in->dims.data(), (int)in->dims.size(), in->data.size());
   float* dG = (float*)tD->data.data();
   double E = 0;
-  std::vector<double> h1(n.h1), h2(n.h2), g1(n.h1), g2(n.h2);
   const int nslot = (int)n.slot_type.size();
-  for (size_t a = 0; a < natom; ++a) {
+  // serial, as the reference configures its TF session (intra/inter-op threads 1, pair_nnp.cpp:23-24)
+  for (long a = 0; a < (long)natom; ++a) {
+    std::vector<double> h1(n.h1), h2(n.h2), g1(n.h1), g2(n.h2);
     const int t = n.slot_type[a % nslot];
     const float* g = G + a * n.din;
     const std::vector<double>&A1 = n.A1[t], &c1 = n.c1[t], &A2 = n.A2[t], &c2 = n.c2[t], &A3 = n.A3[t];
