@@ -193,8 +193,10 @@ int nnpe_nnp_info(nnpe_ctx* ctx, int* din, int* kind);
 int64_t nnpe_nnp_pairs(nnpe_ctx* ctx);
 
 /* Self-test of the tcgen05 tile path on `device`: D[128][N] = bf16(A[128][K]) x bf16(B[N][K])^T,
- * FP32 accumulation in tensor memory (16 <= N <= 256, 16 <= K <= 128, multiples of 16). */
-int nnpe_tc_selftest(int device, int N, int K, const float* A, const float* B, float* D);
+ * FP32 accumulation in tensor memory (16 <= N <= 256, 16 <= K <= 128, multiples of 16).
+ * mode 0: both operands K-major; 1: B MN-major; 2: A rows repeat with period 8 (one 8-row group
+ * addressed with a zero stride); 3: modes 1 and 2 together. */
+int nnpe_tc_selftest(int device, int mode, int N, int K, const float* A, const float* B, float* D);
 
 /* ---- profiling ------------------------------------------------------------------------
  * Enqueue one kernel class without synchronising (for event timing): 0 pair force, 1 list

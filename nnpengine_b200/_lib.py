@@ -78,7 +78,7 @@ _SIGS = {
     "nnpe_nnp_pairs": (C.c_int64, [_vp]),
     "nnpe_bonded_autogen": (C.c_int, [_vp, C.c_int, _f32p, C.c_int, _f32p, C.c_int, _f32p]),
     "nnpe_profile_enqueue": (C.c_int, [_vp, C.c_int]),
-    "nnpe_tc_selftest": (C.c_int, [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p]),
+    "nnpe_tc_selftest": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p]),
     "nnpe_launches_per_step": (C.c_int, [_vp]),
     "nnpe_gr_setup": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int]),
     "nnpe_gr_tally": (C.c_int, [_vp, C.c_int]),

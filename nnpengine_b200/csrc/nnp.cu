@@ -408,6 +408,31 @@ __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_desc_f32(NnpArgs a) {
 
 // ---- embedding force (FP32): recompute the pair's embedding, back-propagate
 // a_c = scale*(dE/dG_i + dE/dG_j)[s*e2+c] through it to dE/dr, fpair = -dE/dr / r.
+// d/dr of sum_c scale * (ga + gb)[c] * y_c(r) * cff(r) for the embedding net wt (W1 b1 W2 b2).
+__device__ __forceinline__ float emb_dedr(const float* wt, int E2, float u, float r_rc, float cff, float dcff,
+                                          float scale, const float* ga, const float* gb) {
+  float h[32], t[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) { h[q] = tanhf(wt[q] * u + wt[32 + q]); t[q] = 0.f; }
+  const float* W2 = wt + 64;
+  const float* b2 = W2 + 32 * E2;
+  float dEdr = 0.f;
+  for (int cc = 0; cc < E2; ++cc) {
+    float z = b2[cc];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) z += h[q] * W2[q * E2 + cc];
+    const float y = tanhf(z);
+    const float ac = scale * (gb ? ga[cc] + gb[cc] : ga[cc]);
+    dEdr += ac * y * dcff;
+    const float g = ac * cff * (1.f - y * y);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) t[q] += g * W2[q * E2 + cc];
+  }
+#pragma unroll
+  for (int q = 0; q < 32; ++q) dEdr += t[q] * (1.f - h[q] * h[q]) * wt[q] * r_rc;
+  return dEdr;
+}
+
 template <bool EV>
 __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_force_f32(NnpArgs a) {
   extern __shared__ float sm[];
@@ -423,6 +448,7 @@ __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_force_f32(NnpArgs a) {
   const uint32_t* row = a.list6 + (size_t)i * a.cap6;
   const int n = a.n6[i];
   const float* dGi = a.dG + (size_t)i * 4 * E2;
+  const int ti = a.info[i].y & 0xFF;
   const float r_rc = 1.f / a.rc;
   float fx = 0, fy = 0, fz = 0;
   double w = 0;
@@ -435,29 +461,17 @@ __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_force_f32(NnpArgs a) {
     const float r = sqrtf(rsq);
     const float u = r * r_rc, cf = r - a.rc, den = 1.f + cf * cf;
     const float cff = 1.f - 1.f / den, dcff = 2.f * cf / (den * den);
-    const int s = ent >> 30;
-    const float* wt = W + eb * ((ent >> 27) & 7);
+    const int s = ent >> 30, tj = (ent >> 27) & 7;
     const float* dGj = a.dG + (size_t)owner_of(j, a.N, a.gowner) * 4 * E2 + s * E2;
     const float* dGis = dGi + s * E2;
-    float h[32], t[32];
-#pragma unroll
-    for (int q = 0; q < 32; ++q) { h[q] = tanhf(wt[q] * u + wt[32 + q]); t[q] = 0.f; }
-    const float* W2 = wt + 64;
-    const float* b2 = W2 + 32 * E2;
-    float dEdr = 0.f;
-    for (int cc = 0; cc < E2; ++cc) {
-      float z = b2[cc];
-#pragma unroll
-      for (int q = 0; q < 32; ++q) z += h[q] * W2[q * E2 + cc];
-      const float y = tanhf(z);
-      const float ac = a.scale * (dGis[cc] + dGj[cc]);
-      dEdr += ac * y * dcff;
-      const float g = ac * cff * (1.f - y * y);
-#pragma unroll
-      for (int q = 0; q < 32; ++q) t[q] += g * W2[q * E2 + cc];
+    // the pair sits in G_i through the net of t_j and in G_j through the net of t_i
+    float dEdr;
+    if (tj == ti) {
+      dEdr = emb_dedr(W + eb * tj, E2, u, r_rc, cff, dcff, a.scale, dGis, dGj);
+    } else {
+      dEdr = emb_dedr(W + eb * tj, E2, u, r_rc, cff, dcff, a.scale, dGis, nullptr) +
+             emb_dedr(W + eb * ti, E2, u, r_rc, cff, dcff, a.scale, dGj, nullptr);
     }
-#pragma unroll
-    for (int q = 0; q < 32; ++q) dEdr += t[q] * (1.f - h[q] * h[q]) * wt[q] * r_rc;
     const float fpair = -dEdr / r;
     fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
     if (EV) w += 0.5 * (double)(fpair * rsq);

@@ -1,20 +1,20 @@
 // BF16 tensor-core (tcgen05) path of the radial-embedding network.
 //
 // Three kernels per force evaluation, each issuing its GEMMs as tcgen05.mma from one thread with
-// operands in shared memory (no-swizzle K-major canonical layout, see tc_util.cuh) and FP32
-// accumulators in tensor memory, read back row-per-thread for the epilogues:
+// operands in shared memory (no-swizzle canonical layouts, see tc_util.cuh) and FP32 accumulators
+// in tensor memory, read back row-per-thread for the epilogues. Tiles of the two pair kernels hold
+// up to 128 pairs of one atom, one pair per MMA row (TMEM lane):
 //
-//  k_tc_desc   one atom per 128-row tile (rows = the atom's pairs inside rc): each thread builds its
-//              pair's first embedding layer h1 = tanh(W1*u + b1) into the A tile, block-diagonal
-//              over neighbour species (K = ntype*32), so one MMA chain A x [W2_0; W2_1]^T gives the
-//              second layer for every row whatever its species; epilogue y = tanh(z + b2) * cff,
-//              then a fixed-order column reduction per special class into G_i (no atomics).
+//  k_tc_desc   first layer h1 = tanh(W1 u + b1) per pair into the A tile, block-diagonal over the
+//              neighbour species (plus a one-hot bias slice) so one MMA chain gives every row the
+//              second layer of its own net; epilogue y = scale cff tanh(z); the sum over pairs
+//              into G_i by special class is a second MMA with a one-hot A (no shuffles, no atomics).
 //  k_tc_fit    128 atoms of one species per tile: G -> h1 -> h2 -> E forward and the hand-written
 //              backward dE/dG = ((A3 (1-h2^2)) A2^T (1-h1^2)) A1^T as four MMA chains (N = 128, 128,
 //              128, 256); every activation stays in shared memory between the chains.
-//  k_tc_force  one atom per tile again: recompute z2 (MMA 1), form g_c = a_c cff (1-y_c^2) with
-//              a_c = scale*(dE/dG_i + dE/dG_j) (MMA 2 back through W2), finish dE/dr on the CUDA
-//              cores and reduce fpair*(x_i-x_j) over the tile's rows in a fixed order.
+//  k_tc_force  second layer and its r-derivative per directed pair (two MMAs), the contraction with
+//              the centre's dE/dG_i on the CUDA cores, and the pair force applied to both atoms in
+//              64-bit fixed point (order-independent sums); k_facc_apply adds it to the forces.
 //
 // Every wait on the MMA-completion mbarrier is bounded; on time-out the kernel records
 // NNPE_DEV_TIMEOUT, stops issuing work, frees its tensor memory and returns.
@@ -27,9 +27,9 @@
 #define NNPE_DEV_TIMEOUT 32
 
 struct NnpTc {
-  int Kd = 0;                        // ntype*32: block-diagonal K of the embedding's second layer
-  unsigned char* d_wdesc = nullptr;  // B image, N=64 (channel) x K=Kd: W2_t[q][c] at k=t*32+q
-  unsigned char* d_wblk = nullptr;   // B image, N=Kd x K=64: W2_t[q][c] at n=t*32+q, k=c
+  int Kd = 0;                        // ntype*32
+  unsigned char* d_wdesc = nullptr;  // B image N=64 (channel) x K=80: W2_t[q][c] at k=t*32+q, b2_t[c] at k=64+t
+  unsigned long long* d_facc = nullptr;   // network forces [natom][3], fixed point (2^-32) for order-free sums
   unsigned char* d_fit = nullptr;    // per species: L1 (N128,K256) L2 (128,128) B2 (128,128) B1 (256,128)
   size_t fit_stride = 0;
   float* d_emb_small = nullptr;      // per species: W1[32] b1[32] b2[64]
@@ -53,18 +53,19 @@ __device__ __forceinline__ float tanh_fast(float x) {
 
 struct TcArgs {
   const float4* pos;
+  const int2* info;
   const uint32_t* list6;
   const int* n6;
   const int* gowner;
   const unsigned char* wdesc;
-  const unsigned char* wblk;
+  unsigned long long* facc;
   const float* emb_small;
   float* G;
   const float* dG;
   float4* frc;
   double* watom;
   int* ctrl;
-  int cap6, N, Kd;
+  int cap6, N, Kd, ntype, npos;
   float rc, scale;
 };
 
@@ -74,21 +75,40 @@ __device__ __forceinline__ void copy_image(unsigned char* dst, const unsigned ch
   for (int k = t; k < bytes / 16; k += nt) d[k] = __ldg(s + k);
 }
 
-// Pair row of a tile: geometry, species, first embedding layer into the A tile (block tj).
+// Wait for the MMA chain committed to bar: thread 0 polls the mbarrier (bounded) while the other
+// threads block on the CTA barrier, so waiting warps take no issue slots from other CTAs. Returns
+// false on every thread when the wait timed out, after recording NNPE_DEV_TIMEOUT.
+__device__ __forceinline__ bool cta_wait_mma(uint64_t* bar, uint32_t phase, int* ctrl) {
+  bool got = true;
+  if (threadIdx.x == 0) {
+    got = tc::mbar_wait(bar, phase);
+    if (!got) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
+  }
+  const bool ok = __syncthreads_and(got) != 0;
+  tc::fence_after();
+  return ok;
+}
+
+// Pair of a tile: geometry, species, cutoff factor and its derivative.
 struct PairRow {
   float dx, dy, dz, rsq, r, cff, dcff;
   int s, tj, jo;
   bool valid;
 };
 
-__device__ __forceinline__ PairRow load_pair(const TcArgs& a, int i, float4 xi, int k, int n) {
+// list entry -> position index, kept inside the position array for entries past the atom's
+// count (those rows are fetched ahead of time and discarded)
+__device__ __forceinline__ int entry_j(uint32_t ent, int npos) {
+  const int j = ent & NNPE_J_MASK;
+  return j < npos ? j : 0;
+}
+
+__device__ __forceinline__ PairRow make_pair(const TcArgs& a, float3 xi, uint32_t ent, float3 xj, bool valid) {
   PairRow p;
-  p.valid = k < n;
+  p.valid = valid;
   p.s = 0; p.tj = 0; p.jo = 0; p.dx = p.dy = p.dz = 0.f; p.rsq = 1.f; p.r = 1.f; p.cff = 0.f; p.dcff = 0.f;
-  if (p.valid) {
-    const uint32_t ent = a.list6[(size_t)i * a.cap6 + k];
+  if (valid) {
     const int j = ent & NNPE_J_MASK;
-    const float4 xj = a.pos[j];
     p.dx = xi.x - xj.x; p.dy = xi.y - xj.y; p.dz = xi.z - xj.z;
     p.rsq = p.dx * p.dx + p.dy * p.dy + p.dz * p.dz;
     p.r = sqrtf(p.rsq);
@@ -102,103 +122,214 @@ __device__ __forceinline__ PairRow load_pair(const TcArgs& a, int i, float4 xi, 
   return p;
 }
 
-__device__ __forceinline__ void write_h1_row(unsigned char* sA, int row, int Kd, const PairRow& p, const float* h) {
-  const uint4 zero = make_uint4(0, 0, 0, 0);
-  for (int kb = 0; kb < Kd / 8; ++kb) {
-    uint4 v = zero;
-    if (p.valid && (kb >> 2) == p.tj) v = tc::pack8(h + (kb & 3) * 8);
-    *reinterpret_cast<uint4*>(sA + tc::kmajor_off(row, kb * 8, Kd)) = v;
+// Per-species embedding constants in shared memory, row stride 129 floats so that the two
+// species' rows fall in different banks: W1 [0,32), b1 [32,64), b2 [64,128).
+constexpr int kEmbStride = 129;
+__device__ __forceinline__ void load_emb(float* sE, const float* emb_small, int ntype, int t, int nt) {
+  for (int k = t; k < 2 * 128; k += nt) sE[(k >> 7) * kEmbStride + (k & 127)] = (k >> 7) < ntype ? emb_small[k] : 0.f;
+}
+
+// 16 first-layer units [q0, q0+16) of species sp's net at u = r/rc: h = tanh(W1 u + b1), and
+// v = dh/dr = (1 - h^2) W1 / rc when V.
+template <bool V>
+__device__ __forceinline__ void first_layer16(const float* sE, int sp, float u, float r_rc, int q0, bool on, float* h,
+                                              float* v) {
+  const float* e = sE + sp * kEmbStride;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const float w1 = e[q0 + q];
+    const float hq = on ? tanh_fast(w1 * u + e[32 + q0 + q]) : 0.f;
+    h[q] = hq;
+    if (V) v[q] = on ? (1.f - hq * hq) * w1 * r_rc : 0.f;
   }
 }
 
+constexpr int kTile = 128;   // pairs per tile (MMA rows)
+// K of the embedding's second-layer MMAs: the first layer in the block of the pair's species
+// ([0, 32) species 0, [32, 64) species 1) and a one-hot bias slice [64, 80) that adds b2_t.
+constexpr int kKE = 80;
+
+// Tile walk of the pair kernels: a CTA owns atoms [i0, i1) and visits their pairs in tiles of up
+// to kTile (one atom per tile). Row p's list entry and neighbour position for the next tile are
+// fetched while the current tile computes.
+struct TileCursor {
+  int i, base, n;
+  float3 xi;
+  uint32_t ent;
+  float3 xj;
+};
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ void cursor_next(const TcArgs& a, const TileCursor& c, int i1, int p, TileCursor& nx,
+                                            bool& more) {
+  nx.i = c.i; nx.base = c.base + kTile; nx.n = c.n; nx.xi = c.xi;
+  if (nx.base >= c.n) { nx.i = c.i + 1; nx.base = 0; }
+  more = nx.i < i1;
+  nx.ent = 0;
+  if (more) {
+    nx.ent = a.list6[(size_t)nx.i * a.cap6 + nx.base + p];
+    if (nx.i != c.i) { nx.n = a.n6[nx.i]; nx.xi = xyz(a.pos[nx.i]); }
+  }
+}
+__device__ __forceinline__ void cursor_first(const TcArgs& a, int i0, int p, TileCursor& c) {
+  c.i = i0; c.base = 0; c.n = a.n6[i0]; c.xi = xyz(a.pos[i0]);
+  c.ent = a.list6[(size_t)i0 * a.cap6 + p];
+  c.xj = xyz(a.pos[entry_j(c.ent, a.npos)]);
+}
+
+// Row p of an A tile [128 x kKE]: 16 values at k0 of the species block sp, zeros at the same
+// offset of the other block; with bias, the one-hot of sp in the bias slice (else zeros).
+__device__ __forceinline__ void put_row16(unsigned char* tile, int p, int sp, int k0, const float* v) {
+  *reinterpret_cast<uint4*>(tile + tc::kmajor_off(p, 32 * sp + k0, kKE)) = tc::pack8(v);
+  *reinterpret_cast<uint4*>(tile + tc::kmajor_off(p, 32 * sp + k0 + 8, kKE)) = tc::pack8(v + 8);
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  *reinterpret_cast<uint4*>(tile + tc::kmajor_off(p, 32 * (1 - sp) + k0, kKE)) = z;
+  *reinterpret_cast<uint4*>(tile + tc::kmajor_off(p, 32 * (1 - sp) + k0 + 8, kKE)) = z;
+}
+__device__ __forceinline__ void put_bias(unsigned char* tile, int p, int sp, bool one) {
+  uint4 u = make_uint4(0, 0, 0, 0);
+  if (one) {   // bf16 1.0 in element sp of the first 8
+    const uint32_t v = 0x3F80u << (16 * (sp & 1));
+    if (sp < 2) u.x = v; else u.y = v;
+  }
+  *reinterpret_cast<uint4*>(tile + tc::kmajor_off(p, 64, kKE)) = u;
+  *reinterpret_cast<uint4*>(tile + tc::kmajor_off(p, 72, kKE)) = make_uint4(0, 0, 0, 0);
+}
+
 // -------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_tc_desc(TcArgs a) {
-  extern __shared__ __align__(1024) unsigned char sm[];
+// Descriptor. Tile = up to 128 pairs of one atom i, pair p in MMA row / TMEM lane p = thread p.
+//  MMA 1: Z = H1 W2s + b2, H1 [128 x 80] holding each pair's first layer in the block of its
+//         neighbour species plus the one-hot bias slice, W2s = [W2_0; W2_1; b2] (K = 80, N = 64):
+//         row p of Z is the second-layer input of the net of t_p.
+//  epilogue: Y[p][c] = scale cff_p tanh(Z[p][c]), rounded to BF16, written over the H1 tile
+//         (which MMA 1 has consumed).
+//  MMA 2: G_i[s][c] = sum_p S[s][p] Y[p][c], S the one-hot of the pair's special class: A = S
+//         (8 rows, read with zero row-group stride so every 8-row group of the M = 128 tile
+//         repeats it), B = Y (MN-major), K = the tile's pairs. Lanes 0..3 of the accumulator
+//         then hold G_i by class, in FP32.
+// Rows past the atom's pairs are neither computed nor read (H1 rows past the count only feed
+// unread accumulator rows; Y rows up to the 16-pair MMA granule are written as zeros).
+constexpr int kSmemDesc = 64 * kKE * 2 + kTile * kKE * 2 + 8 * kTile * 2 + 2 * kEmbStride * 4;
+__global__ void __launch_bounds__(128, 8) k_tc_desc(TcArgs a) {
+  extern __shared__ __align__(128) unsigned char sm[];   // no-swizzle operands need 16-byte alignment
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
-  const int Kd = a.Kd;
-  unsigned char* sW = sm;
-  unsigned char* sA = sW + 64 * Kd * 2;
-  float* sY = reinterpret_cast<float*>(sA + 128 * Kd * 2);   // [128][65]
-  int* sS = reinterpret_cast<int*>(sY + 128 * 65);
-  const int t = threadIdx.x, w = t >> 5;
+  unsigned char* sW = sm;                        // B of MMA 1: N = 64 channels x K = 80
+  unsigned char* sHY = sW + 64 * kKE * 2;        // A of MMA 1 (128 pairs x K = 80), then B of MMA 2
+  unsigned char* sS = sHY + kTile * kKE * 2;     // A of MMA 2: 8 classes x K = 128 pairs
+  float* sE = reinterpret_cast<float*>(sS + 8 * kTile * 2);   // embedding constants (8 CTAs per SM fit)
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31, p = t;
   if (w == 0) tc::tmem_alloc(&tmem_base, 64);
   if (t == 0) tc::mbar_init(&bar, 1);
-  copy_image(sW, a.wdesc, 64 * Kd * 2, t, 128);
+  copy_image(sW, a.wdesc, 64 * kKE * 2, t, 128);
+  load_emb(sE, a.emb_small, a.ntype, t, 128);
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = tmem_base;
   const uint32_t taddr = tmem + ((uint32_t)(w * 32) << 16);
-  const uint32_t idesc = tc::idesc_bf16(128, 64);
-  const uint32_t aA = tc::smem_u32(sA), aW = tc::smem_u32(sW);
-  const int col = t & 63, half = t >> 6;
+  const uint32_t aW = tc::smem_u32(sW), aHY = tc::smem_u32(sHY), aS = tc::smem_u32(sS);
   const float r_rc = 1.f / a.rc;
   uint32_t phase = 0;
   bool alive = true;
   const int per = (a.N + gridDim.x - 1) / gridDim.x;
   const int i0 = blockIdx.x * per, i1 = min(a.N, i0 + per);
-  for (int i = i0; i < i1 && alive; ++i) {
-    const float4 xi = a.pos[i];
-    const int n = a.n6[i];
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int base = 0; base < n && alive; base += 128) {
-      const PairRow p = load_pair(a, i, xi, base + t, n);
-      float h[32];
-      const float* es = a.emb_small + p.tj * 128;
-      const float u = p.r * r_rc;
+  TileCursor cur;
+  if (i0 < i1) cursor_first(a, i0, p, cur);
+  bool more = i0 < i1;
+  while (more && alive) {
+    TileCursor nx;
+    cursor_next(a, cur, i1, p, nx, more);
+    const int cnt = max(0, min(kTile, cur.n - cur.base)), NK = (cnt + 15) & ~15;
+    const PairRow pr = make_pair(a, cur.xi, cur.ent, cur.xj, p < cnt);
+    if (pr.valid) {
+      const float u = pr.r * r_rc;
 #pragma unroll
-      for (int q = 0; q < 32; ++q) h[q] = tanh_fast(es[q] * u + es[32 + q]);
-      write_h1_row(sA, t, Kd, p, h);
-      sS[t] = p.s;
-      tc::fence_async_smem();
-      tc::fence_before();
-      __syncthreads();
-      tc::fence_after();
-      if (t == 0) {
-        for (int kk = 0; kk < Kd / 16; ++kk)
-          tc::mma_bf16(tmem, tc::tile_desc(aA, Kd, kk), tc::tile_desc(aW, Kd, kk), idesc, kk > 0);
-        tc::mma_commit(&bar);
+      for (int hq = 0; hq < 2; ++hq) {
+        float h[16];
+        first_layer16<false>(sE, pr.tj, u, r_rc, 16 * hq, true, h, nullptr);
+        put_row16(sHY, p, pr.tj, 16 * hq, h);
       }
-      {
-        const bool got = tc::mbar_wait(&bar, phase);
-        alive = __syncthreads_and(got) != 0;   // CTA-uniform: every thread takes the same path
-        if (!got && (t & 31) == 0) atomicOr(a.ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
-      }
-      phase ^= 1;
-      tc::fence_after();
-      if (alive) {
-        const float cs = p.valid ? a.scale * p.cff : 0.f;
+      put_bias(sHY, p, pr.tj, true);
+    }
+    if (p < NK) {
+      const uint16_t one = 0x3F80u;
 #pragma unroll
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-          float v[16];
-          tc::tmem_ld16(taddr + c0, v);
+      for (int c = 0; c < 8; ++c)
+        *reinterpret_cast<uint16_t*>(sS + tc::kmajor_off(c, p, kTile)) = (pr.valid && pr.s == c) ? one : (uint16_t)0;
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (t == 0) {
+      const uint32_t id = tc::idesc_bf16(128, 64);
+      for (int kk = 0; kk < kKE / 16; ++kk)
+        tc::mma_bf16(tmem, tc::tile_desc(aHY, kKE, kk), tc::tile_desc(aW, kKE, kk), id, kk > 0);
+      tc::mma_commit(&bar);
+    }
+    alive = cta_wait_mma(&bar, phase, a.ctrl);
+    phase ^= 1;
+    nx.xj = more ? xyz(a.pos[entry_j(nx.ent, a.npos)]) : make_float3(0.f, 0.f, 0.f);
+    if (alive && 32 * w < NK) {   // warp-uniform
+      const float cs = a.scale * pr.cff;   // 0 for rows past the atom's pairs
 #pragma unroll
-          for (int q = 0; q < 16; ++q) sY[t * 65 + c0 + q] = tanh_fast(v[q] + es[64 + c0 + q]) * cs;
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        float z[16], z2[16];
+        tc::tmem_ld16x2(taddr + c0, taddr + c0 + 16, z, z2);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          z[q] = pr.valid ? tanh_fast(z[q]) * cs : 0.f;
+          z2[q] = pr.valid ? tanh_fast(z2[q]) * cs : 0.f;
+        }
+        if (p < NK) {
+          *reinterpret_cast<uint4*>(sHY + tc::mnmajor_off(c0, p, 64)) = tc::pack8(z);
+          *reinterpret_cast<uint4*>(sHY + tc::mnmajor_off(c0 + 8, p, 64)) = tc::pack8(z + 8);
+          *reinterpret_cast<uint4*>(sHY + tc::mnmajor_off(c0 + 16, p, 64)) = tc::pack8(z2);
+          *reinterpret_cast<uint4*>(sHY + tc::mnmajor_off(c0 + 24, p, 64)) = tc::pack8(z2 + 8);
         }
       }
-      tc::fence_before();
-      __syncthreads();
-      const int rows = min(128, n - base);
-      for (int rr = 0; rr < 64; ++rr) {
-        const int row = half * 64 + rr;
-        if (row >= rows) break;
-        const float v = sY[row * 65 + col];
-        const int sc = sS[row];
-        acc[0] += sc == 0 ? v : 0.f;
-        acc[1] += sc == 1 ? v : 0.f;
-        acc[2] += sc == 2 ? v : 0.f;
-        acc[3] += sc == 3 ? v : 0.f;
-      }
-      __syncthreads();
     }
-    // combine the two row halves and store G_i[s*64+c]
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    float* Gi = a.G + (size_t)cur.i * 256;
+    if (NK > 0) {   // CTA-uniform
+      if (alive && t == 0) {
+        const uint32_t id = tc::idesc_bf16(128, 64, true);
+        for (int kk = 0; kk < NK / 16; ++kk)
+          tc::mma_bf16(tmem, tc::tile_desc_bcast(aS, kTile, kk), tc::tile_desc_mn(aHY, 64, kk), id, kk > 0);
+        tc::mma_commit(&bar);
+      }
+      if (alive) alive = cta_wait_mma(&bar, phase, a.ctrl);
+      phase ^= 1;
+      if (alive && w == 0) {   // lanes 0..3 hold G_i by special class
 #pragma unroll
-    for (int sc = 0; sc < 4; ++sc) sY[(half * 4 + sc) * 64 + col] = acc[sc];
+        for (int c0 = 0; c0 < 64; c0 += 32) {
+          float g[16], g2[16];
+          tc::tmem_ld16x2(tmem + c0, tmem + c0 + 16, g, g2);
+          if (lane < 4) {
+            float4* dst = reinterpret_cast<float4*>(Gi + lane * 64 + c0);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float* src = q < 4 ? g + 4 * q : g2 + 4 * (q - 4);
+              float4 v = make_float4(src[0], src[1], src[2], src[3]);
+              if (cur.base > 0) {
+                const float4 o = dst[q];
+                v.x += o.x; v.y += o.y; v.z += o.z; v.w += o.w;
+              }
+              dst[q] = v;
+            }
+          }
+        }
+      }
+    } else if (cur.base == 0) {
+      for (int e = t; e < 256; e += 128) Gi[e] = 0.f;   // an atom without pairs
+    }
+    tc::fence_before();
     __syncthreads();
-    for (int e = t; e < 256; e += 128) a.G[(size_t)i * 256 + e] = sY[e] + sY[256 + e];
-    __syncthreads();
+    cur = nx;
   }
   tc::fence_before();
   __syncthreads();
@@ -206,149 +337,160 @@ __global__ void __launch_bounds__(128) k_tc_desc(TcArgs a) {
 }
 
 // -------------------------------------------------------------------------------------------
+// Force. The pair (i, j) enters G_i through the net of t_j and G_j through the net of t_i, so
+// dE/dr_ij = T(i->j) + T(j->i) with T(i->j) = scale sum_c dE/dG_i[s*64+c] d(y_c cff)/dr, y the
+// net of t_j. Each directed pair of the full list computes its own T from the centre's dE/dG_i
+// (one net per pair, no gather of dE/dG_j) and applies fpair = -T/r with opposite signs to i and
+// to j's owner; the reverse visit supplies the other half. Forces are summed in 64-bit fixed
+// point (2^-32), whose integer additions give the same bits in any order, and added to the
+// FP32 forces by k_facc_apply.
+//  MMA 1: Z = H W2s + b2 (as in the descriptor), MMA 2: K = V W2s, V = dh1/dr in the same
+//  block layout with a zero bias slice, so K[p][c] = dz2_c/dr.
+//  epilogue: thread (p, half) takes 32 channels: with a = dE/dG_i[s][c] and y = tanh(z),
+//  d(y cff)/dr = y dcff + cff (1 - y^2) kappa, so T = scale (dcff sum a y + cff sum a kappa (1 - y^2)).
+// The per-atom virial gets -T r for each of the atom's directed pairs.
+// Tensor memory: Z in columns [0, 64), K in [64, 128).
+constexpr int kSmemForce = 64 * kKE * 2 + 2 * kTile * kKE * 2 + 256 * 4 + 2 * kTile * 4 + 2 * kEmbStride * 4;
+constexpr float kFix = 4294967296.f;   // fixed-point scale of the network forces
+
+__device__ __forceinline__ void fix_add(unsigned long long* dst, float v) {
+  atomicAdd(dst, (unsigned long long)__float2ll_rn(v * kFix));
+}
+
 template <bool EV>
-__global__ void __launch_bounds__(128) k_tc_force(TcArgs a) {
-  extern __shared__ __align__(1024) unsigned char sm[];
+__global__ void __launch_bounds__(256, 4) k_tc_force(TcArgs a) {
+  extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
-  __shared__ float sRed[4][4];
-  const int Kd = a.Kd;
-  unsigned char* sW1 = sm;                          // N=64 x K=Kd
-  unsigned char* sW2 = sW1 + 64 * Kd * 2;           // N=Kd x K=64
-  unsigned char* sA = sW2 + Kd * 64 * 2;            // 128 x Kd
-  unsigned char* sA2 = sA + 128 * Kd * 2;           // 128 x 64
-  float* sdGi = reinterpret_cast<float*>(sA2 + 128 * 64 * 2);   // 256
+  __shared__ float sRed[4][3];
+  __shared__ double sVir[4];
+  unsigned char* sW = sm;                                        // B: N = 64 x K = 80
+  unsigned char* sH = sW + 64 * kKE * 2;                         // A of MMA 1
+  unsigned char* sV = sH + kTile * kKE * 2;                      // A of MMA 2
+  float* sdGi = reinterpret_cast<float*>(sV + kTile * kKE * 2);  // dE/dG_i [256]
+  float* sAcc = sdGi + 256;                                      // [2][128]: per-half sums
+  float* sE = sAcc + 2 * kTile;
   const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-  const uint32_t ncols = 64 + Kd <= 128 ? 128 : 256;
-  if (w == 0) tc::tmem_alloc(&tmem_base, ncols);
+  const int p = ((w & 3) << 5) | lane, half = w >> 2;   // pair row, channel half of this thread
+  if (w == 0) tc::tmem_alloc(&tmem_base, 128);
   if (t == 0) tc::mbar_init(&bar, 1);
-  copy_image(sW1, a.wdesc, 64 * Kd * 2, t, 128);
-  copy_image(sW2, a.wblk, Kd * 64 * 2, t, 128);
+  copy_image(sW, a.wdesc, 64 * kKE * 2, t, 256);
+  load_emb(sE, a.emb_small, a.ntype, t, 256);
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = tmem_base;
-  const uint32_t taddr = tmem + ((uint32_t)(w * 32) << 16);
-  const uint32_t id1 = tc::idesc_bf16(128, 64), id2 = tc::idesc_bf16(128, Kd);
-  const uint32_t aA = tc::smem_u32(sA), aA2 = tc::smem_u32(sA2), aW1 = tc::smem_u32(sW1), aW2 = tc::smem_u32(sW2);
+  const uint32_t taddr = tmem + ((uint32_t)((w & 3) * 32) << 16);
+  const uint32_t aW = tc::smem_u32(sW), aH = tc::smem_u32(sH), aV = tc::smem_u32(sV);
   const float r_rc = 1.f / a.rc;
   uint32_t phase = 0;
   bool alive = true;
   const int per = (a.N + gridDim.x - 1) / gridDim.x;
   const int i0 = blockIdx.x * per, i1 = min(a.N, i0 + per);
-  for (int i = i0; i < i1 && alive; ++i) {
-    const float4 xi = a.pos[i];
-    const int n = a.n6[i];
-    for (int e = t; e < 256; e += 128) sdGi[e] = a.dG[(size_t)i * 256 + e];
-    float fx = 0.f, fy = 0.f, fz = 0.f, vir = 0.f;
-    for (int base = 0; base < n && alive; base += 128) {
-      const PairRow p = load_pair(a, i, xi, base + t, n);
-      float h[32];
-      const float* es = a.emb_small + p.tj * 128;
-      const float u = p.r * r_rc;
-#pragma unroll
-      for (int q = 0; q < 32; ++q) h[q] = tanh_fast(es[q] * u + es[32 + q]);
-      write_h1_row(sA, t, Kd, p, h);
-      tc::fence_async_smem();
-      tc::fence_before();
-      __syncthreads();
-      tc::fence_after();
-      if (t == 0) {
-        for (int kk = 0; kk < Kd / 16; ++kk)
-          tc::mma_bf16(tmem, tc::tile_desc(aA, Kd, kk), tc::tile_desc(aW1, Kd, kk), id1, kk > 0);
-        tc::mma_commit(&bar);
-      }
-      {
-        const bool got = tc::mbar_wait(&bar, phase);
-        alive = __syncthreads_and(got) != 0;
-        if (!got && lane == 0) atomicOr(a.ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
-      }
-      phase ^= 1;
-      tc::fence_after();
-      float dEdr = 0.f;
-      if (alive) {
-        const float* dGj = a.dG + (size_t)p.jo * 256 + p.s * 64;
-        const float* dGi = sdGi + p.s * 64;
-#pragma unroll
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-          float v[16], g[16];
-          tc::tmem_ld16(taddr + c0, v);
-#pragma unroll
-          for (int q = 0; q < 16; q += 4) {
-            float4 dj = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (p.valid) dj = *reinterpret_cast<const float4*>(dGj + c0 + q);
-            const float dd[4] = {dj.x, dj.y, dj.z, dj.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int c = c0 + q + e;
-              const float y = tanh_fast(v[q + e] + es[64 + c]);
-              const float ac = a.scale * (dGi[c] + dd[e]);
-              dEdr += ac * y * p.dcff;
-              g[q + e] = p.valid ? ac * p.cff * (1.f - y * y) : 0.f;
-            }
-          }
-          *reinterpret_cast<uint4*>(sA2 + tc::kmajor_off(t, c0, 64)) = tc::pack8(g);
-          *reinterpret_cast<uint4*>(sA2 + tc::kmajor_off(t, c0 + 8, 64)) = tc::pack8(g + 8);
-        }
-      }
-      tc::fence_async_smem();
-      tc::fence_before();
-      __syncthreads();
-      tc::fence_after();
-      if (alive && t == 0) {
-        for (int kk = 0; kk < 4; ++kk)
-          tc::mma_bf16(tmem + 64, tc::tile_desc(aA2, 64, kk), tc::tile_desc(aW2, 64, kk), id2, kk > 0);
-        tc::mma_commit(&bar);
-      }
-      if (alive) {
-        const bool got = tc::mbar_wait(&bar, phase);
-        alive = __syncthreads_and(got) != 0;
-        if (!got && lane == 0) atomicOr(a.ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
-      }
-      phase ^= 1;
-      tc::fence_after();
-      if (alive) {
-        for (int k16 = 0; k16 < Kd / 16; ++k16) {
-          float v[16];
-          tc::tmem_ld16(taddr + 64 + k16 * 16, v);
-          if ((k16 >> 1) == p.tj) {
-#pragma unroll
-            for (int q = 0; q < 16; ++q) {
-              const int qq = (k16 & 1) * 16 + q;
-              dEdr += v[q] * (1.f - h[qq] * h[qq]) * es[qq] * r_rc;
-            }
-          }
-        }
-        if (p.valid) {
-          const float fpair = -dEdr / p.r;
-          fx += p.dx * fpair; fy += p.dy * fpair; fz += p.dz * fpair;
-          if (EV) vir += 0.5f * fpair * p.rsq;
-        }
-      }
-      tc::fence_before();
-      __syncthreads();
+  TileCursor cur;
+  if (i0 < i1) cursor_first(a, i0, p, cur);
+  bool more = i0 < i1;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  double vir = 0.0;
+  while (more && alive) {
+    TileCursor nx;
+    cursor_next(a, cur, i1, p, nx, more);
+    if (cur.base == 0) sdGi[t] = a.dG[(size_t)cur.i * 256 + t];
+    const int cnt = max(0, min(kTile, cur.n - cur.base));
+    const PairRow pr = make_pair(a, cur.xi, cur.ent, cur.xj, p < cnt);
+    if (pr.valid) {
+      float h[16], v[16];
+      first_layer16<true>(sE, pr.tj, pr.r * r_rc, r_rc, 16 * half, true, h, v);
+      put_row16(sH, p, pr.tj, 16 * half, h);
+      put_row16(sV, p, pr.tj, 16 * half, v);
+      if (half == 0) { put_bias(sH, p, pr.tj, true); put_bias(sV, p, pr.tj, false); }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      fx += __shfl_xor_sync(0xffffffffu, fx, o);
-      fy += __shfl_xor_sync(0xffffffffu, fy, o);
-      fz += __shfl_xor_sync(0xffffffffu, fz, o);
-      vir += __shfl_xor_sync(0xffffffffu, vir, o);
-    }
-    if (lane == 0) { sRed[w][0] = fx; sRed[w][1] = fy; sRed[w][2] = fz; sRed[w][3] = vir; }
+    tc::fence_async_smem();
+    tc::fence_before();
     __syncthreads();
+    tc::fence_after();
     if (t == 0) {
-      const float4 f = a.frc[i];
-      a.frc[i] = make_float4(f.x + ((sRed[0][0] + sRed[1][0]) + (sRed[2][0] + sRed[3][0])),
-                             f.y + ((sRed[0][1] + sRed[1][1]) + (sRed[2][1] + sRed[3][1])),
-                             f.z + ((sRed[0][2] + sRed[1][2]) + (sRed[2][2] + sRed[3][2])), f.w);
-      if (EV) a.watom[i] += (double)((sRed[0][3] + sRed[1][3]) + (sRed[2][3] + sRed[3][3]));
+      const uint32_t id = tc::idesc_bf16(128, 64);
+      for (int kk = 0; kk < kKE / 16; ++kk)
+        tc::mma_bf16(tmem, tc::tile_desc(aH, kKE, kk), tc::tile_desc(aW, kKE, kk), id, kk > 0);
+      for (int kk = 0; kk < kKE / 16; ++kk)
+        tc::mma_bf16(tmem + 64, tc::tile_desc(aV, kKE, kk), tc::tile_desc(aW, kKE, kk), id, kk > 0);
+      tc::mma_commit(&bar);
     }
+    alive = cta_wait_mma(&bar, phase, a.ctrl);
+    phase ^= 1;
+    nx.xj = more ? xyz(a.pos[entry_j(nx.ent, a.npos)]) : make_float3(0.f, 0.f, 0.f);
+    float sy = 0.f, sk = 0.f;
+    if (alive && 32 * (w & 3) < cnt) {   // warp-uniform: the loads below are warp-collective
+      const float* ag = sdGi + pr.s * 64 + 32 * half;
+#pragma unroll
+      for (int c0 = 0; c0 < 32; c0 += 16) {
+        float z[16], kap[16];
+        tc::tmem_ld16x2(taddr + 32 * half + c0, taddr + 64 + 32 * half + c0, z, kap);
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) {
+          const float4 a4 = *reinterpret_cast<const float4*>(ag + c0 + q);
+          const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float y = tanh_fast(z[q + e]);
+            sy = fmaf(av[e], y, sy);
+            sk = fmaf(av[e] * kap[q + e], fmaf(-y, y, 1.f), sk);
+          }
+        }
+      }
+    }
+    sAcc[half * kTile + p] = pr.valid ? a.scale * (pr.dcff * sy + pr.cff * sk) : 0.f;
     __syncthreads();
+    if (half == 0 && pr.valid) {
+      const float fpair = -(sAcc[p] + sAcc[kTile + p]) / pr.r;
+      const float gx = pr.dx * fpair, gy = pr.dy * fpair, gz = pr.dz * fpair;
+      fx += gx; fy += gy; fz += gz;
+      unsigned long long* fj = a.facc + 3 * (size_t)pr.jo;
+      fix_add(fj, -gx); fix_add(fj + 1, -gy); fix_add(fj + 2, -gz);
+      if (EV) vir += (double)(fpair * pr.rsq);
+    }
+    if (!more || nx.i != cur.i) {   // CTA-uniform: last tile of atom cur.i
+      if (w < 4) {
+        for (int o = 16; o > 0; o >>= 1) {
+          fx += __shfl_xor_sync(0xffffffffu, fx, o);
+          fy += __shfl_xor_sync(0xffffffffu, fy, o);
+          fz += __shfl_xor_sync(0xffffffffu, fz, o);
+          if (EV) vir += __shfl_xor_sync(0xffffffffu, vir, o);
+        }
+        if (lane == 0) { sRed[w][0] = fx; sRed[w][1] = fy; sRed[w][2] = fz; sVir[w] = vir; }
+      }
+      __syncthreads();
+      if (t == 0 && cur.n > 0) {
+        unsigned long long* fi = a.facc + 3 * (size_t)cur.i;
+        fix_add(fi, (sRed[0][0] + sRed[1][0]) + (sRed[2][0] + sRed[3][0]));
+        fix_add(fi + 1, (sRed[0][1] + sRed[1][1]) + (sRed[2][1] + sRed[3][1]));
+        fix_add(fi + 2, (sRed[0][2] + sRed[1][2]) + (sRed[2][2] + sRed[3][2]));
+        if (EV) a.watom[cur.i] += (sVir[0] + sVir[1]) + (sVir[2] + sVir[3]);
+      }
+      fx = fy = fz = 0.f;
+      vir = 0.0;
+    }
+    tc::fence_before();
+    __syncthreads();
+    cur = nx;
   }
   tc::fence_before();
   __syncthreads();
-  if (w == 0) tc::tmem_dealloc(tmem, ncols);
+  if (w == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+// frc[i] += fixed-point network force of atom i
+__global__ void k_facc_apply(const unsigned long long* __restrict__ facc, float4* __restrict__ frc, int N) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double s = 1.0 / kFix;
+  float4 f = frc[i];
+  f.x += (float)((double)(long long)facc[3 * i] * s);
+  f.y += (float)((double)(long long)facc[3 * i + 1] * s);
+  f.z += (float)((double)(long long)facc[3 * i + 2] * s);
+  frc[i] = f;
 }
 
 // -------------------------------------------------------------------------------------------
@@ -377,11 +519,7 @@ __device__ __forceinline__ bool fit_mma(uint32_t tmem, uint32_t aA, int KA, uint
     for (int kk = 0; kk < KA / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(aA, KA, kk), tc::tile_desc(aB, KA, kk), id, kk > 0);
     tc::mma_commit(bar);
   }
-  const bool got = tc::mbar_wait(bar, phase);
-  const bool ok = __syncthreads_and(got) != 0;
-  if (!got && (t & 31) == 0) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
-  tc::fence_after();
-  return ok;
+  return cta_wait_mma(bar, phase, ctrl);
 }
 
 __device__ __forceinline__ void sync_image(unsigned char* sW, const unsigned char* src, int bytes, int t) {
@@ -391,7 +529,7 @@ __device__ __forceinline__ void sync_image(unsigned char* sW, const unsigned cha
 }
 
 __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
-  extern __shared__ __align__(1024) unsigned char sm[];
+  extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
   unsigned char* sAct = sm;                 // 128 x 256 (G), later 128 x 128 (g2)
@@ -516,7 +654,7 @@ void put_image(std::vector<uint16_t>& img, size_t base, int N, int K, F&& val) {
 void nnp_tc_free(NnpModel* m) {
   NnpTc* t = m->tc;
   if (!t) return;
-  for (void* p : {(void*)t->d_wdesc, (void*)t->d_wblk, (void*)t->d_fit, (void*)t->d_emb_small, (void*)t->d_fit_small,
+  for (void* p : {(void*)t->d_wdesc, (void*)t->d_facc, (void*)t->d_fit, (void*)t->d_emb_small, (void*)t->d_fit_small,
                   (void*)t->d_tile_sp, (void*)t->d_tile_row, (void*)t->d_soff})
     if (p) cudaFree(p);
   delete t;
@@ -526,16 +664,19 @@ void nnp_tc_free(NnpModel* m) {
 // Weight images and tile tables for the tensor-core path (embedding 1->32->64, fitting 256->128->128).
 int nnp_tc_setup(nnpe_ctx* c) {
   NnpModel* m = c->nnp;
-  if (m->kind != 1 || m->e1 != 32 || m->e2 != 64 || m->h1 != 128 || m->h2 != 128) return 0;   // FP32 only
+  // the tensor-core kernels hold every species' net side by side in K = 64 / N = 128: at most 2 species
+  if (m->kind != 1 || m->e1 != 32 || m->e2 != 64 || m->h1 != 128 || m->h2 != 128 || c->ntype > 2) return 0;
   auto* t = new NnpTc();
   m->tc = t;
   const int T = c->ntype, Kd = 32 * T;
   t->Kd = Kd;
   const size_t eb = 32 + 32 + 32 * 64 + 64;
   const float* E = m->h_embw.data();
-  std::vector<uint16_t> wdesc((size_t)64 * Kd), wblk((size_t)Kd * 64);
-  put_image(wdesc, 0, 64, Kd, [&](int n, int k) { return E[eb * (k / 32) + 64 + (k % 32) * 64 + n]; });
-  put_image(wblk, 0, Kd, 64, [&](int n, int k) { return E[eb * (n / 32) + 64 + (n % 32) * 64 + k]; });
+  std::vector<uint16_t> wdesc((size_t)64 * kKE);
+  put_image(wdesc, 0, 64, kKE, [&](int n, int k) {
+    if (k < 64) return k / 32 < T ? E[eb * (k / 32) + 64 + (k % 32) * 64 + n] : 0.f;
+    return k - 64 < T ? E[eb * (k - 64) + 64 + 32 * 64 + n] : 0.f;   // bias rows b2_t
+  });
   std::vector<float> emb_small((size_t)T * 128);
   for (int s = 0; s < T; ++s)
     for (int q = 0; q < 32; ++q) {
@@ -574,15 +715,14 @@ int nnp_tc_setup(nnpe_ctx* c) {
     return 0;
   };
   if (int rc = up((void**)&t->d_wdesc, wdesc.data(), wdesc.size() * 2)) return rc;
-  if (int rc = up((void**)&t->d_wblk, wblk.data(), wblk.size() * 2)) return rc;
+  NNPE_CUDA(c, cudaMalloc((void**)&t->d_facc, sizeof(unsigned long long) * 3 * std::max(c->natom, 1)));
   if (int rc = up((void**)&t->d_fit, fit.data(), fit.size() * 2)) return rc;
   if (int rc = up((void**)&t->d_emb_small, emb_small.data(), emb_small.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_fit_small, fit_small.data(), fit_small.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_tile_sp, tsp.data(), tsp.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_tile_row, trow.data(), trow.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_soff, m->soff.data(), m->soff.size() * 4)) return rc;
-  const int smem_desc = 64 * Kd * 2 + 128 * Kd * 2 + 128 * 65 * 4 + 128 * 4;
-  const int smem_force = 64 * Kd * 2 + Kd * 64 * 2 + 128 * Kd * 2 + 128 * 64 * 2 + 256 * 4;
+  const int smem_desc = kSmemDesc, smem_force = kSmemForce;
   const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 256 * 128 * 2;
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_desc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_desc));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
@@ -597,29 +737,30 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   if (!t) return nnpe_fail(c, NNPE_EARG, "BF16 tensor-core path needs the 1->32->64 / 256->128->128 network");
   const int Kd = t->Kd;
   TcArgs a;
-  a.pos = c->d_pos; a.list6 = m->d_list6; a.n6 = m->d_n6; a.gowner = c->d_gowner; a.wdesc = t->d_wdesc; a.wblk = t->d_wblk;
+  a.pos = c->d_pos; a.info = c->d_info; a.list6 = m->d_list6; a.n6 = m->d_n6; a.gowner = c->d_gowner; a.wdesc = t->d_wdesc; a.facc = t->d_facc;
   a.emb_small = t->d_emb_small; a.G = m->d_G; a.dG = m->d_dG; a.frc = c->d_frc; a.watom = c->d_watom; a.ctrl = c->d_ctrl;
-  a.cap6 = m->cap6; a.N = c->natom; a.Kd = Kd; a.rc = m->rc; a.scale = m->scale;
+  a.cap6 = m->cap6; a.N = c->natom; a.Kd = Kd; a.ntype = c->ntype; a.npos = c->natom + c->Gcap; a.rc = m->rc; a.scale = m->scale;
   const int sms = nnpe_sm_count(c->device);
-  const int smem_desc = 64 * Kd * 2 + 128 * Kd * 2 + 128 * 65 * 4 + 128 * 4;
-  const int smem_force = 64 * Kd * 2 + Kd * 64 * 2 + 128 * Kd * 2 + 128 * 64 * 2 + 256 * 4;
   const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 256 * 128 * 2;
-  k_tc_desc<<<std::min(c->natom, sms * 3), 128, smem_desc, c->stream>>>(a);
+  k_tc_desc<<<std::min(c->natom, sms * 8), 128, kSmemDesc, c->stream>>>(a);
   FitTcArgs f;
   f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row; f.G = m->d_G;
   f.fit = t->d_fit; f.fit_stride = t->fit_stride; f.small = t->d_fit_small; f.dG = m->d_dG; f.enet = m->d_enet;
   f.ctrl = c->d_ctrl;
   k_tc_fit<<<t->ntiles, 128, smem_fit, c->stream>>>(f);
-  if (ev) k_tc_force<true><<<std::min(c->natom, sms * 4), 128, smem_force, c->stream>>>(a);
-  else k_tc_force<false><<<std::min(c->natom, sms * 4), 128, smem_force, c->stream>>>(a);
+  NNPE_CUDA(c, cudaMemsetAsync(t->d_facc, 0, sizeof(unsigned long long) * 3 * c->natom, c->stream));
+  if (ev) k_tc_force<true><<<std::min(c->natom, sms * 4), 256, kSmemForce, c->stream>>>(a);
+  else k_tc_force<false><<<std::min(c->natom, sms * 4), 256, kSmemForce, c->stream>>>(a);
+  k_facc_apply<<<(c->natom + 255) / 256, 256, 0, c->stream>>>(t->d_facc, c->d_frc, c->natom);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }
 
 namespace {
 // One CTA: D[128][N] = bf16(A[128][K]) x bf16(B[N][K])^T with FP32 accumulation in TMEM.
+// mode 0: A, B K-major; mode 1: B MN-major; mode 2: A row-broadcast (rows repeat every 8, SBO=0).
 __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A, const float* __restrict__ B,
-                                                     float* __restrict__ D, int N, int K, int ncols, int* err) {
+                                                     float* __restrict__ D, int N, int K, int ncols, int mode, int* err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
@@ -628,32 +769,47 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
   unsigned char* sB = smraw + 128 * K * 2;
   if (w == 0) tc::tmem_alloc(&tmem_base, ncols);
   if (t == 0) tc::mbar_init(&bar, 1);
-  for (int k = 0; k < K; k += 8) {
-    float f[8];
-    for (int q = 0; q < 8; ++q) f[q] = A[t * K + k + q];
-    *reinterpret_cast<uint4*>(sA + tc::kmajor_off(t, k, K)) = tc::pack8(f);
-  }
-  for (int r = t; r < N; r += 128)
+  const bool a_bcast = mode == 2 || mode == 3, b_mn = mode == 1 || mode == 3;
+  if (!a_bcast || t < 8)
     for (int k = 0; k < K; k += 8) {
       float f[8];
-      for (int q = 0; q < 8; ++q) f[q] = B[r * K + k + q];
-      *reinterpret_cast<uint4*>(sB + tc::kmajor_off(r, k, K)) = tc::pack8(f);
+      for (int q = 0; q < 8; ++q) f[q] = A[t * K + k + q];
+      *reinterpret_cast<uint4*>(sA + tc::kmajor_off(t, k, K)) = tc::pack8(f);
     }
+  if (b_mn) {
+    // MN-major: thread handles (k, 8 consecutive n) chunks
+    for (int e = t; e < K * (N / 8); e += 128) {
+      const int k = e / (N / 8), n0 = (e % (N / 8)) * 8;
+      float f[8];
+      for (int q = 0; q < 8; ++q) f[q] = B[(n0 + q) * K + k];
+      *reinterpret_cast<uint4*>(sB + tc::mnmajor_off(n0, k, N)) = tc::pack8(f);
+    }
+  } else {
+    for (int r = t; r < N; r += 128)
+      for (int k = 0; k < K; k += 8) {
+        float f[8];
+        for (int q = 0; q < 8; ++q) f[q] = B[r * K + k + q];
+        *reinterpret_cast<uint4*>(sB + tc::kmajor_off(r, k, K)) = tc::pack8(f);
+      }
+  }
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tbase = tmem_base;
   if (t == 0) {
-    const uint32_t idesc = tc::idesc_bf16(128, N);
-    for (int kk = 0; kk < K / 16; ++kk)
-      tc::mma_bf16(tbase, tc::tile_desc(tc::smem_u32(sA), K, kk), tc::tile_desc(tc::smem_u32(sB), K, kk), idesc, kk > 0);
+    const uint32_t idesc = tc::idesc_bf16(128, N, b_mn);
+    for (int kk = 0; kk < K / 16; ++kk) {
+      const uint64_t ad = a_bcast ? tc::tile_desc_bcast(tc::smem_u32(sA), K, kk) : tc::tile_desc(tc::smem_u32(sA), K, kk);
+      const uint64_t bd = b_mn ? tc::tile_desc_mn(tc::smem_u32(sB), N, kk) : tc::tile_desc(tc::smem_u32(sB), K, kk);
+      tc::mma_bf16(tbase, ad, bd, idesc, kk > 0);
+    }
     tc::mma_commit(&bar);
   }
   const bool ok = tc::mbar_wait(&bar, 0);
   if (!ok && (t & 31) == 0) atomicOr(err, 1);
   tc::fence_after();
-  if (ok) {
+  if (__syncthreads_and(ok)) {
     for (int c0 = 0; c0 < N; c0 += 16) {
       float v[16];
       tc::tmem_ld16(tbase + ((uint32_t)(w * 32) << 16) + c0, v);
@@ -667,8 +823,8 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
 }  // namespace
 
 // Self-test of the tcgen05 tile path: D[128][N] = A[128][K] x B[N][K]^T with BF16 operands.
-extern "C" int nnpe_tc_selftest(int device, int N, int K, const float* A, const float* B, float* D) {
-  if (N < 16 || N > 256 || N % 16 || K < 16 || K > 128 || K % 16 || !A || !B || !D) return NNPE_EARG;
+extern "C" int nnpe_tc_selftest(int device, int mode, int N, int K, const float* A, const float* B, float* D) {
+  if (N < 16 || N > 256 || N % 16 || K < 16 || K > 128 || K % 16 || !A || !B || !D || mode < 0 || mode > 3) return NNPE_EARG;
   if (cudaSetDevice(device) != cudaSuccess) return NNPE_ECUDA;
   float *dA, *dB, *dD;
   int* derr;
@@ -682,7 +838,7 @@ extern "C" int nnpe_tc_selftest(int device, int N, int K, const float* A, const 
   cudaMemset(derr, 0, sizeof(int));
   const int smem = (128 + N) * K * 2;
   cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k_tc_selftest<<<1, 128, smem>>>(dA, dB, dD, N, K, ncols, derr);
+  k_tc_selftest<<<1, 128, smem>>>(dA, dB, dD, N, K, ncols, mode, derr);
   cudaError_t e = cudaDeviceSynchronize();
   int herr = 0;
   cudaMemcpy(D, dD, sizeof(float) * 128 * N, cudaMemcpyDeviceToHost);

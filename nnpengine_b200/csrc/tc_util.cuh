@@ -33,9 +33,25 @@ __device__ __forceinline__ uint64_t tile_desc(uint32_t saddr, int K, int kk) {
   return sdesc(saddr + 256u * kk, 128u, (uint32_t)(K >> 3) * 128u);
 }
 
-// instruction descriptor: kind::f16, A=B=BF16, D=F32, both K-major, shape M x N
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// instruction descriptor: kind::f16, A=B=BF16, D=F32, shape M x N; A and B K-major unless
+// b_mn (bit 16) selects an MN-major B operand
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool b_mn = false) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// MN-major no-swizzle tile [N rows (MN) x K]: core matrix (n/8, k/8) holds 8 K-rows of 8 contiguous
+// MN elements; MN-adjacent core matrices are 128 B apart (SBO), K-adjacent ones (N/8)*128 B (LBO).
+__device__ __forceinline__ uint32_t mnmajor_off(int n, int k, int N) {
+  return ((uint32_t)(((k >> 3) * (N >> 3) + (n >> 3)) << 7)) + ((k & 7) << 4) + ((n & 7) << 1);
+}
+__device__ __forceinline__ uint64_t tile_desc_mn(uint32_t saddr, int N, int kk) {
+  return sdesc(saddr + 2u * (uint32_t)(N >> 3) * 128u * kk, (uint32_t)(N >> 3) * 128u, 128u);
+}
+// K-major descriptor whose 8-row groups all alias the first one (SBO = 0): an M x K operand whose
+// rows repeat with period 8, held in 8*K*2 bytes
+__device__ __forceinline__ uint64_t tile_desc_bcast(uint32_t saddr, int K, int kk) {
+  return sdesc(saddr + 256u * kk, 128u, 0u);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
@@ -98,6 +114,38 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 #pragma unroll
   for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
+
+// 2 x 16 FP32 columns (at ta and tb) of this thread's lane behind one wait; the wait names the
+// destination registers so no use of them can be scheduled before it.
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va, float* vb) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(ta));
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(tb));
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]),
+                 "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]),
+                 "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) { va[k] = __uint_as_float(r[k]); vb[k] = __uint_as_float(r[16 + k]); }
+}
+
+// 16-byte global -> shared copy that bypasses L1 (cp.async), and the wait for this thread's copies
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // 8 floats -> 8 bf16 packed in a 16-byte chunk
 __device__ __forceinline__ uint4 pack8(const float* f) {

@@ -633,14 +633,34 @@ int orc_nnp_tbl(const orc_t* o, double cutoff_d, int nbin, const float* coef_p, 
   return 0;
 }
 
+/* d/dr of sum_c a_c * scale * y_c(r) * cff(r) for the embedding net at W1 (W1, b1, W2, b2 in a row),
+ * with h and t scratch of e1 + e2 and e1 entries. */
+static real emb_dedr(const float* W1, int e1, int e2, real u, real r_rc, real cff, real dcff, real scale,
+                     const real* a, real* h, real* t) {
+  const float *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
+  for (int q = 0; q < e1; ++q) { h[q] = tanh((real)W1[q] * u + (real)b1[q]); t[q] = 0; }
+  real dEdr = 0;
+  for (int c = 0; c < e2; ++c) {
+    real z = (real)b2[c];
+    for (int q = 0; q < e1; ++q) z += h[q] * (real)W2[(size_t)q * e2 + c];
+    real yc = tanh(z), ac = scale * a[c];
+    dEdr += ac * yc * dcff;
+    real gc = ac * cff * (1 - yc * yc);
+    for (int q = 0; q < e1; ++q) t[q] += gc * (real)W2[(size_t)q * e2 + c];
+  }
+  for (int q = 0; q < e1; ++q) dEdr += t[q] * (1 - h[q] * h[q]) * (real)W1[q] * r_rc;
+  return dEdr;
+}
+
 /* Radial-embedding NNP (the network of the 96k-atom workload; no counterpart in the reference's
  * C++, whose network sits behind TF). Per neighbour species t_j an embedding net
  * u=r/rc -> e1 (tanh) -> e2 (tanh); the pair's contribution scale*y_c(r)*cff(r), with the
  * reference's cutoff factor cff = 1-1/(1+(r-rc)^2) (pair_nnp.cpp:573-584), is accumulated into
  * descriptor slot s*e2+c of atom i by special class s (the reference selects its descriptor
  * functions by special class the same way, pair_nnp.cpp:663); a per-species fitting network on
- * the 4*e2 inputs gives E_i; forces follow the reference's back-projection
- * fpair = -sum_c (dE/dG_i + dE/dG_j)[s*e2+c] d(phi_c)/dr / r (pair_nnp.cpp:753-764).
+ * the 4*e2 inputs gives E_i. Forces follow the reference's back-projection (pair_nnp.cpp:753-764),
+ * fpair = -dE/dr / r with dE/dr = sum_c dE/dG_i[s*e2+c] d(phi^{t_j}_c)/dr + dE/dG_j[s*e2+c]
+ * d(phi^{t_i}_c)/dr: the pair sits in G_i through the net of t_j and in G_j through that of t_i.
  * Embedding block per species: W1[e1] b1[e1] W2[e1][e2] b2[e2]. */
 int orc_nnp_emb(const orc_t* o, double cutoff_d, double scale_d, int e1, int e2, const float* embw, int h1, int h2,
                 const float* fitw, double* G_out, double* dEdG_out, double* e_atom, double* f_by_id,
@@ -692,21 +712,10 @@ int orc_nnp_emb(const orc_t* o, double cutoff_d, double scale_d, int e1, int e2,
       if (!(rsq < cutsq)) continue;
       real r = sqrt(rsq), u = r * r_rc;
       int s = special_of(o, ia, ja);
-      const float *W1 = embw + eb * o->typ[ja], *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
       real cf = r - rc, den = 1 + cf * cf, cff = 1 - 1 / den, dcff = 2 * cf / (den * den);
-      for (int a = 0; a < e1; ++a) h[a] = tanh((real)W1[a] * u + (real)b1[a]);
-      real dEdr = 0;
-      for (int a = 0; a < e1; ++a) t[a] = 0;
-      for (int c = 0; c < e2; ++c) {
-        real z = (real)b2[c];
-        for (int a = 0; a < e1; ++a) z += h[a] * (real)W2[(size_t)a * e2 + c];
-        real yc = tanh(z);
-        real ac = scale * (dG[(size_t)ia * din + s * e2 + c] + dG[(size_t)ja * din + s * e2 + c]);
-        dEdr += ac * yc * dcff;
-        real gc = ac * cff * (1 - yc * yc);
-        for (int a = 0; a < e1; ++a) t[a] += gc * (real)W2[(size_t)a * e2 + c];
-      }
-      for (int a = 0; a < e1; ++a) dEdr += t[a] * (1 - h[a] * h[a]) * (real)W1[a] * r_rc;
+      /* dE/dr_ij: G_i holds y_{t_j}(r) and G_j holds y_{t_i}(r), both in slot s */
+      real dEdr = emb_dedr(embw + eb * o->typ[ja], e1, e2, u, r_rc, cff, dcff, scale, dG + (size_t)ia * din + s * e2, h, t) +
+                  emb_dedr(embw + eb * o->typ[ia], e1, e2, u, r_rc, cff, dcff, scale, dG + (size_t)ja * din + s * e2, h, t);
       real fpair = -dEdr / r;
       fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
       w += 0.5 * (double)(fpair * rsq);

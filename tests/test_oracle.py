@@ -114,3 +114,28 @@ def test_restated_nnp_tbl_matches_reference():
     fb, _, _ = o.bonded(*[np.asarray(x) * np.array([1, 2, 1, 2], np.float32) for x in cases.water_bonded_raw()[:2]],
                         np.zeros((1, 4), np.float32))
     assert cases.rel_rms(r["f"] + fb, g["force"]) < 1e-5
+
+
+def test_embedding_nnp_forces_are_energy_gradient():
+    """The FP64 oracle's embedding-network forces equal -dE/dx by central differences, on
+    atoms of both species (a pair enters G_i through the net of t_j and G_j through that of t_i)."""
+    from nnpengine_b200 import nnp_model as NM
+    s, _ = cases.water_case(jitter=0.05)
+    m = NM.embed_model()
+    o = orc.Restated(s, "f64")
+
+    def run(x):
+        assert o.rebuild(x, 6, 2, 8) == 0
+        return o.nnp_emb(6.0, m.scale, m.e1, m.e2, m.embw, m.h1, m.h2, m.fitw)
+
+    x0 = s.x.astype(np.float32)
+    f = run(x0)["f"]
+    h = np.float32(2e-3)
+    for atom in (0, 1, 2, 301):
+        for d in range(3):
+            xp, xm = x0.copy(), x0.copy()
+            xp[atom, d] += h
+            xm[atom, d] -= h
+            step = float(xp[atom, d]) - float(xm[atom, d])
+            grad = (run(xp)["e_net"] - run(xm)["e_net"]) / step
+            assert abs(grad + f[atom, d]) < 2e-4 * np.abs(f[atom]).max() + 1e-6, (atom, d, grad, f[atom, d])
