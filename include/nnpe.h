@@ -147,6 +147,15 @@ int nnpe_compute_forces(nnpe_ctx* ctx, int ev, double* erg, double* virial);
  * with the list check and rebuild of run.cpp:236-283 done on the device first. Writes the forces
  * to f_host (atom-id order); erg/virial (FP64) when non-NULL. */
 int nnpe_force_step(nnpe_ctx* ctx, const float* x_host, float* f_host, double* erg, double* virial);
+/* nnpe_force_step without any device allocation; no counterpart in the reference. Positions and
+ * forces are staged in a statically reserved device array (3 MiB on every GPU that loads the
+ * library, held until exit) instead of buffers allocated on first use, for callers that cannot let
+ * the library allocate: a run loop whose process reserves the device's memory for its own
+ * allocator, or one that cannot take the implicit inter-stream synchronisation of an allocation.
+ * natom <= 131072, else NNPE_EARG. The first call on a device looks up the array's address with
+ * that device current: make it before any stream capture. All contexts on a device share the
+ * array, so calls that overlap in time race on it; serialise them. */
+int nnpe_force_step_noalloc(nnpe_ctx* ctx, const float* x_host, float* f_host, double* erg, double* virial);
 /* Forces (kind 0) or accelerations after the last step (kind 1), atom-id order [natom*3]. */
 int nnpe_get_forces(nnpe_ctx* ctx, int kind, float* f);
 int nnpe_get_positions(nnpe_ctx* ctx, float* x);

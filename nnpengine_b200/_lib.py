@@ -61,6 +61,7 @@ _SIGS = {
     "nnpe_compute_forces": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nnpe_get_forces": (C.c_int, [_vp, C.c_int, _f32p]),
     "nnpe_force_step": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "nnpe_force_step_noalloc": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nnpe_get_positions": (C.c_int, [_vp, _f32p]),
     "nnpe_get_positions_f64": (C.c_int, [_vp, _f64p]),
     "nnpe_get_velocities": (C.c_int, [_vp, _f32p]),

@@ -24,6 +24,7 @@ UNITS = {
     "ctx.cu": EXACT,
     "rebuild.cu": EXACT,
     "forces.cu": EXACT,
+    "force_step_noalloc.cu": EXACT,
     "integrate.cu": EXACT,
     "gr.cu": EXACT,
     "nnp.cu": [],
