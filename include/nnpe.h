@@ -51,6 +51,7 @@ typedef struct nnpe_thermo {
   double temperature; /* ekin/natom*ek_T [K] */
   double pressure;    /* (virial+2 ekin)/3 * ev_GPa / BL^3 [GPa] */
   double erg_nnp;     /* network part of erg */
+  double erg_exp;     /* RMDF penalty of the last g(r) step (run.cpp:295, 386), 0 without RMDF */
 } nnpe_thermo;
 
 /* ---- context -------------------------------------------------------------------------- */
@@ -225,6 +226,28 @@ int nnpe_gr_nbin(const nnpe_ctx* ctx, int inner);
  * (reduce_local grsq.cpp:207-219 with a double normaliser); sq [npair][nq] in FP64. */
 int nnpe_gr_get(nnpe_ctx* ctx, int inner, uint64_t* counts, double* gr);
 int nnpe_sq_compute(nnpe_ctx* ctx, int inner, double* sq, double* q);
+
+/* ---- RMDF (grsq.h:82-112): reverse-MD / FMIRL refinement of the pair table ---------------
+ * RMDF ctor (grsq.cpp:899-1059) from arrays: n_sq targets, per q point (the SQ grid) S_exp, the
+ * weight wt (multiplied by strength) and ntype scattering factors ff[n][q][t]. gamma = 1 is DA/RMD,
+ * 0 <= gamma < 1 FMIRL. Refines LJTableCoulDSF's table when the pair term is on, else the network
+ * term's pair tables (RMDF(..., nullptr, &nnp), run.cpp:1059). The table and g(r) grids must agree
+ * ("RMDF mismatch", grsq.cpp:926-947). The table as it stands is kept as the base. Once set, every
+ * g(r) step of nnpe_run/nnpe_run_graph runs compute_Qspace + compute_Rspace after S(q), and
+ * compute_Potential on log steps when gamma != 1 (run.cpp:286-299). */
+int nnpe_rmdf_set(nnpe_ctx* ctx, int n_sq, const double* sqex, const double* wt, const double* ff, double strength,
+                  double gamma);
+/* The same from the reference's target files: nq lines "q S_exp wt f_0 ... f_{ntype-1}". */
+int nnpe_rmdf_load(nnpe_ctx* ctx, int n_sq, const char* const* files, double strength, double gamma);
+/* RMDF::loadDeltaSQ (grsq.cpp:1419-1443); a missing file is ignored, as there. */
+int nnpe_rmdf_load_delta(nnpe_ctx* ctx, const char* fname);
+/* One update on the current S(q): compute_Qspace, compute_Rspace, compute_Potential if potential;
+ * erg_exp = the penalty times natom/4 (grsq.cpp:1117). */
+int nnpe_rmdf_step(nnpe_ctx* ctx, int potential, double* erg_exp);
+/* Weighted S_n(q), deltaS_n(q) [n_sq][nq] and force_q [npair][nq] of the last update (NULL to skip). */
+int nnpe_rmdf_get(nnpe_ctx* ctx, double* sq, double* deltasq, double* force_q);
+/* RMDF::dumpSQ (grsq.cpp:1380-1416). */
+int nnpe_rmdf_dump_sq(nnpe_ctx* ctx, const char* fname, int append);
 
 #ifdef __cplusplus
 }

@@ -23,7 +23,7 @@ _vp = C.c_void_p
 class Thermo(C.Structure):
     _fields_ = [("step", C.c_int), ("nbuild", C.c_int), ("erg", C.c_double), ("virial", C.c_double),
                 ("ekin", C.c_double), ("temperature", C.c_double), ("pressure", C.c_double),
-                ("erg_nnp", C.c_double)]
+                ("erg_nnp", C.c_double), ("erg_exp", C.c_double)]
 
 
 _SIGS = {
@@ -86,6 +86,12 @@ _SIGS = {
     "nnpe_gr_nbin": (C.c_int, [_vp, C.c_int]),
     "nnpe_gr_get": (C.c_int, [_vp, C.c_int, _u64p, _f64p]),
     "nnpe_sq_compute": (C.c_int, [_vp, C.c_int, _f64p, _f64p]),
+    "nnpe_rmdf_set": (C.c_int, [_vp, C.c_int, _f64p, _f64p, _f64p, C.c_double, C.c_double]),
+    "nnpe_rmdf_load": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_char_p), C.c_double, C.c_double]),
+    "nnpe_rmdf_load_delta": (C.c_int, [_vp, C.c_char_p]),
+    "nnpe_rmdf_step": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
+    "nnpe_rmdf_get": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "nnpe_rmdf_dump_sq": (C.c_int, [_vp, C.c_char_p, C.c_int]),
 }
 
 _lib = None

@@ -27,6 +27,7 @@ UNITS = {
     "force_step_noalloc.cu": EXACT,
     "integrate.cu": EXACT,
     "gr.cu": EXACT,
+    "rmdf.cu": EXACT,
     "nnp.cu": [],
     "nnp_tc.cu": [],
 }

@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(1024) k_reduce(const double* eatom, const doub
       const int slot = ctrl[CTRL_NLOG];
       if (slot < log_cap) {
         LogRec r;
-        r.erg = e + en; r.virial = w; r.ekin = with_kin ? k : red[2]; r.erg_nnp = en;
+        r.erg = e + en; r.virial = w; r.ekin = with_kin ? k : red[2]; r.erg_nnp = en; r.erg_exp = red[4];
         r.step = ctrl[CTRL_STEP]; r.nbuild = ctrl[CTRL_NBUILD]; r.pad0 = r.pad1 = 0;
         log[slot] = r;
       }

@@ -190,10 +190,21 @@ int gr_tally_enqueue(nnpe_ctx* c, int inner) {
   return 0;
 }
 
-static int sq_enqueue(nnpe_ctx* c, int inner) {
-  const int P = c->npair, nbin = inner ? c->gr_nbin_inner : c->gr_nbin;
-  k_gr_norm<<<nblocks((long)P * nbin, 256), 256, 0, c->stream>>>(inner ? c->d_gr_counts_inner : c->d_gr_counts,
-                                                                  c->d_gr_norm, c->d_gr, P, nbin);
+// GR::tally<true> clears and fills only the first nbin_r_inner bins of the per-thread counts
+// (grsq.cpp:96-105); the bins beyond keep the last cell-based tally, and reduce_local/SQ::compute
+// read all nbin_r bins (grsq.cpp:207-219, 299-322). The list-based counts are therefore copied
+// over the first bins of the full-range counts, which then hold exactly the reference's sums.
+static int merge_inner_enqueue(nnpe_ctx* c) {
+  const size_t w = sizeof(unsigned long long);
+  NNPE_CUDA(c, cudaMemcpy2DAsync(c->d_gr_counts, w * c->gr_nbin, c->d_gr_counts_inner, w * c->gr_nbin_inner,
+                                 w * c->gr_nbin_inner, c->npair, cudaMemcpyDeviceToDevice, c->stream));
+  return 0;
+}
+
+// g(r) over the full range and S(q) from it (SQ::compute uses gr->nbin_r bins, grsq.cpp:282).
+static int sq_enqueue(nnpe_ctx* c) {
+  const int P = c->npair, nbin = c->gr_nbin;
+  k_gr_norm<<<nblocks((long)P * nbin, 256), 256, 0, c->stream>>>(c->d_gr_counts, c->d_gr_norm, c->d_gr, P, nbin);
   const double dr = (double)c->gr_dr;
   const double rho = (double)c->natom / std::pow((double)c->grid.bl, 3);
   k_sq<<<c->gr_nq, 256, 0, c->stream>>>(c->d_gr, c->d_sq, c->d_qq, P, nbin, c->gr_nq, dr, c->gr_qmax / c->gr_nq,
@@ -202,11 +213,17 @@ static int sq_enqueue(nnpe_ctx* c, int inner) {
   return 0;
 }
 
-int gr_step_enqueue(nnpe_ctx* c, bool long_tally) {
+int rmdf_step_enqueue(nnpe_ctx* c, bool potential);
+
+// One g(r) step of the loop (run.cpp:286-299): tally, g(r), S(q), then the RMDF table update.
+int gr_step_enqueue(nnpe_ctx* c, bool long_tally, bool rmdf_potential) {
   const int inner = long_tally ? 0 : 1;
   if (int rc = gr_tally_enqueue(c, inner)) return rc;
+  if (inner)
+    if (int rc = merge_inner_enqueue(c)) return rc;
   c->gr_tallied = inner;
-  return sq_enqueue(c, inner);
+  if (int rc = sq_enqueue(c)) return rc;
+  return rmdf_step_enqueue(c, rmdf_potential);
 }
 
 int nnpe_sync_errors(nnpe_ctx* c);
@@ -215,6 +232,8 @@ extern "C" int nnpe_gr_tally(nnpe_ctx* c, int inner) {
   if (!c || !c->have_setup || !c->d_gr_counts) return nnpe_fail(c, NNPE_EARG, "nnpe_gr_tally: no g(r) set up");
   cudaSetDevice(c->device);
   if (int rc = gr_tally_enqueue(c, inner ? 1 : 0)) return rc;
+  if (inner)
+    if (int rc = merge_inner_enqueue(c)) return rc;
   c->gr_tallied = inner ? 1 : 0;
   return nnpe_sync_errors(c);
 }
@@ -239,7 +258,8 @@ extern "C" int nnpe_gr_get(nnpe_ctx* c, int inner, uint64_t* counts, double* gr)
 extern "C" int nnpe_sq_compute(nnpe_ctx* c, int inner, double* sq, double* q) {
   if (!c || !c->d_gr_counts) return nnpe_fail(c, NNPE_EARG, "nnpe_sq_compute: no g(r) set up");
   cudaSetDevice(c->device);
-  if (int rc = sq_enqueue(c, inner ? 1 : 0)) return rc;
+  (void)inner;   // S(q) always spans the full g(r) range, as SQ::compute
+  if (int rc = sq_enqueue(c)) return rc;
   if (sq) NNPE_CUDA(c, cudaMemcpyAsync(sq, c->d_sq, sizeof(double) * c->npair * c->gr_nq, cudaMemcpyDeviceToHost, c->stream));
   if (q) NNPE_CUDA(c, cudaMemcpyAsync(q, c->d_qq, sizeof(double) * c->gr_nq, cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -8,7 +8,8 @@
 
 int check_valid_enqueue(nnpe_ctx* c);
 int nnpe_sync_errors(nnpe_ctx* c);
-int gr_step_enqueue(nnpe_ctx* c, bool long_tally);
+int gr_step_enqueue(nnpe_ctx* c, bool long_tally, bool rmdf_potential);
+bool rmdf_potential_on_log(const nnpe_ctx* c);
 
 namespace {
 
@@ -196,7 +197,8 @@ static int enqueue_step(nnpe_ctx* c, int variant) {
   if (int rc = rebuild_enqueue(c, true)) return rc;
   if (int rc = ghost_update_enqueue(c, true)) return rc;
   if (gr)
-    if (int rc = gr_step_enqueue(c, gr_long)) return rc;
+    // run.cpp:298: the potential table is refreshed on log steps when gamma != 1
+    if (int rc = gr_step_enqueue(c, gr_long, f_log && rmdf_potential_on_log(c))) return rc;
   if (int rc = forces_enqueue(c, f_log)) return rc;
   if (int rc = verlet_v_enqueue(c, f_log || thermo)) return rc;
   if (f_log || thermo) {
@@ -262,6 +264,7 @@ static int finish_run(nnpe_ctx* c, nnpe_thermo* log, int max_log, int* nlog) {
       nnpe_thermo& t = log[k];
       t.step = h[k].step; t.nbuild = h[k].nbuild; t.erg = h[k].erg; t.virial = h[k].virial; t.ekin = h[k].ekin;
       t.erg_nnp = h[k].erg_nnp;
+      t.erg_exp = h[k].erg_exp;
       t.temperature = t.ekin / c->natom * kEkT;                                 // run.cpp:380
       t.pressure = (t.virial + t.ekin * 2) / 3 * kEvGPa / vol;                   // run.cpp:381
     }

@@ -48,11 +48,12 @@ struct Stencil {
 };
 
 struct LogRec {
-  double erg, virial, ekin, erg_nnp;
+  double erg, virial, ekin, erg_nnp, erg_exp;
   int step, nbuild, pad0, pad1;
 };
 
 struct NnpModel;   // network term (nnp.cu)
+struct RmdfState;  // structure-factor refinement (rmdf.cu)
 
 struct nnpe_ctx {
   int device = 0;
@@ -142,6 +143,8 @@ struct nnpe_ctx {
   bool force_step_init = false;
   // network term
   NnpModel* nnp = nullptr;
+  // RMDF refinement of the pair table (d_red[4] holds the last erg_exp)
+  RmdfState* rmdf = nullptr;
   // CUDA graphs of the step variants
   cudaGraphExec_t graph_exec[16] = {};
   bool graph_valid = false;
@@ -214,3 +217,4 @@ int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
 int nnp_forces_enqueue(nnpe_ctx* c, bool ev);
 int nnpe_bonded_coefs(nnpe_ctx* c, const float* bcoef, const float* acoef, const float* dcoef);
 void nnp_free(nnpe_ctx* c);
+void rmdf_free(nnpe_ctx* c);

@@ -38,6 +38,7 @@ struct NnpTc {
   int* d_tile_row = nullptr;
   int ntiles = 0;
   int* d_soff = nullptr;
+  int ctas_desc = 1, ctas_force = 1;   // resident CTAs per SM (shared memory, registers, tensor memory)
 };
 
 namespace {
@@ -728,6 +729,12 @@ int nnp_tc_setup(nnpe_ctx* c) {
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fit));
+  // one wave of resident CTAs: a grid larger than what fits leaves a partial second wave
+  int od = 0, of = 0;
+  NNPE_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, k_tc_desc, 128, smem_desc));
+  NNPE_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&of, k_tc_force<true>, 256, smem_force));
+  t->ctas_desc = std::max(1, std::min(od, 512 / 64));
+  t->ctas_force = std::max(1, std::min(of, 512 / 128));
   return 0;
 }
 
@@ -742,15 +749,16 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   a.cap6 = m->cap6; a.N = c->natom; a.Kd = Kd; a.ntype = c->ntype; a.npos = c->natom + c->Gcap; a.rc = m->rc; a.scale = m->scale;
   const int sms = nnpe_sm_count(c->device);
   const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 256 * 128 * 2;
-  k_tc_desc<<<std::min(c->natom, sms * 8), 128, kSmemDesc, c->stream>>>(a);
+  k_tc_desc<<<std::min(c->natom, sms * t->ctas_desc), 128, kSmemDesc, c->stream>>>(a);
   FitTcArgs f;
   f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row; f.G = m->d_G;
   f.fit = t->d_fit; f.fit_stride = t->fit_stride; f.small = t->d_fit_small; f.dG = m->d_dG; f.enet = m->d_enet;
   f.ctrl = c->d_ctrl;
   k_tc_fit<<<t->ntiles, 128, smem_fit, c->stream>>>(f);
   NNPE_CUDA(c, cudaMemsetAsync(t->d_facc, 0, sizeof(unsigned long long) * 3 * c->natom, c->stream));
-  if (ev) k_tc_force<true><<<std::min(c->natom, sms * 4), 256, kSmemForce, c->stream>>>(a);
-  else k_tc_force<false><<<std::min(c->natom, sms * 4), 256, kSmemForce, c->stream>>>(a);
+  const int gforce = std::min(c->natom, sms * t->ctas_force);
+  if (ev) k_tc_force<true><<<gforce, 256, kSmemForce, c->stream>>>(a);
+  else k_tc_force<false><<<gforce, 256, kSmemForce, c->stream>>>(a);
   k_facc_apply<<<(c->natom + 255) / 256, 256, 0, c->stream>>>(t->d_facc, c->d_frc, c->natom);
   NNPE_CHECK_LAUNCH(c);
   return 0;

@@ -112,6 +112,7 @@ class Engine:
             F = np.concatenate([F, np.zeros((F.shape[0], 1), np.float32)], 1)
             U = np.concatenate([U, np.zeros((U.shape[0], 1), np.float32)], 1)
         self._ok(self.lib.nnpe_pair_set_table(self.h, F.shape[1] - 1, _f32(F).ravel(), _f32(U).ravel()))
+        self.nbin = F.shape[1] - 1
 
     def load_pair_table(self, nbin: int, path: str):
         self._ok(self.lib.nnpe_pair_load_table(self.h, nbin, path.encode()))
@@ -264,3 +265,36 @@ class Engine:
         q = np.zeros(self.nq)
         self._ok(self.lib.nnpe_sq_compute(self.h, int(inner), s, q))
         return s.reshape(self.npair, self.nq), q
+
+    # ---- RMDF ------------------------------------------------------------------------------
+    def rmdf_set(self, sqex, wt, ff, strength: float, gamma: float):
+        """sqex, wt: [n_sq][nq]; ff: [n_sq][nq][ntype] (the target files' columns)."""
+        sqex = np.ascontiguousarray(sqex, np.float64).reshape(-1, self.nq)
+        wt = np.ascontiguousarray(wt, np.float64).reshape(-1, self.nq)
+        ff = np.ascontiguousarray(ff, np.float64)
+        self.n_sq = sqex.shape[0]
+        self._ok(self.lib.nnpe_rmdf_set(self.h, self.n_sq, sqex.ravel(), wt.ravel(), ff.ravel(), strength, gamma))
+
+    def rmdf_load(self, files, strength: float, gamma: float):
+        arr = (C.c_char_p * len(files))(*[f.encode() for f in files])
+        self.n_sq = len(files)
+        self._ok(self.lib.nnpe_rmdf_load(self.h, len(files), arr, strength, gamma))
+
+    def rmdf_step(self, potential: bool = False) -> float:
+        e = C.c_double(0)
+        self._ok(self.lib.nnpe_rmdf_step(self.h, int(potential), C.byref(e)))
+        return e.value
+
+    def rmdf_get(self):
+        s = np.zeros(self.n_sq * self.nq)
+        d = np.zeros(self.n_sq * self.nq)
+        f = np.zeros(self.npair * self.nq)
+        self._ok(self.lib.nnpe_rmdf_get(self.h, s.ctypes.data, d.ctypes.data, f.ctypes.data))
+        return s.reshape(self.n_sq, self.nq), d.reshape(self.n_sq, self.nq), f.reshape(self.npair, self.nq)
+
+    def pair_table(self):
+        nb1 = self.nbin + 1
+        F = np.zeros(self.npair * nb1, np.float32)
+        U = np.zeros(self.npair * nb1, np.float32)
+        self._ok(self.lib.nnpe_pair_get_table(self.h, F, U))
+        return F.reshape(self.npair, nb1), U.reshape(self.npair, nb1)

@@ -294,3 +294,24 @@ def write_pair_table(path: str, r, F, U) -> None:
 
 def write_velocity_file(path: str, v: np.ndarray) -> None:
     np.asarray(v, np.float32).tofile(path)
+
+
+def write_sq_target(path: str, q, sqex, wt, ff) -> None:
+    """RMDF target file (grsq.cpp:897): ``q S_exp wt f_0 ... f_{ntype-1}`` per q point, %.9e."""
+    ff = np.asarray(ff, np.float64)
+    with open(path, "w") as f:
+        for i in range(len(q)):
+            f.write(f"{q[i]:.9e} {sqex[i]:.9e} {wt[i]:.9e}" + "".join(f" {v:.9e}" for v in ff[i]) + "\n")
+
+
+def synthetic_sq_target(nq: int = 512, qmax: float = 20.0, ntype: int = 2, q_min: float = 0.3, seed: int = 0):
+    """A smooth seeded stand-in for a measured structure factor on the SQ grid q_i = (i+.5) qmax/nq:
+    S_exp(q) = a sin(b q) exp(-c q), weight 1 from q_min up (0 below), scattering factors constant
+    per type. Returns q, S_exp, wt, ff[nq][ntype] (float32 values, as the reference reads them)."""
+    rng = np.random.default_rng(seed)
+    q = ((np.arange(nq, dtype=np.float32) + np.float32(0.5)) * np.float32(qmax / nq)).astype(np.float32)
+    a, b, c = rng.uniform(0.05, 0.15), rng.uniform(0.8, 1.2), rng.uniform(0.05, 0.15)
+    sqex = (a * np.sin(b * q) * np.exp(-c * q)).astype(np.float32)
+    wt = (q >= q_min).astype(np.float32)
+    ff = np.tile(np.linspace(1.0, 0.6, ntype, dtype=np.float32), (nq, 1))
+    return q, sqex, wt, ff

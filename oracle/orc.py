@@ -200,8 +200,66 @@ def read_ref_dump(d: str) -> Dict[str, np.ndarray]:
                      ("f_classical.f32", np.float32), ("desc.f32", np.float32), ("dedg.f32", np.float32),
                      ("gr_counts.i64", np.int64), ("gr_inner_counts.i64", np.int64), ("gr.f32", np.float32),
                      ("sq.f32", np.float32), ("qq.f32", np.float32), ("rr.f32", np.float32), ("log_e.f64", np.float64),
-                     ("log_w.f64", np.float64), ("log_k.f64", np.float64), ("log_enn.f64", np.float64)]:
+                     ("log_w.f64", np.float64), ("log_k.f64", np.float64), ("log_enn.f64", np.float64),
+                     ("log_exp.f64", np.float64), ("rmdf_erg.f64", np.float64), ("rmdf_sq.f32", np.float32),
+                     ("tbl_force.f32", np.float32), ("tbl_pot.f32", np.float32)]:
         p = os.path.join(d, name)
         if os.path.exists(p):
             out[name.split(".")[0]] = np.fromfile(p, dt)
     return out
+
+
+# ----------------------------------------------------------------------------------------------
+# RMDF restated in FP64 (grsq.cpp:899-1377)
+# ----------------------------------------------------------------------------------------------
+
+def rmdf_setup(typ, ntype, nbin, dr, nq, qmax, sqex, wt, ff, strength):
+    """RMDF ctor (grsq.cpp:899-1059): per target n the weights sqwt/fwt [n][P][nq] from the
+    scattering factors and type counts, wt*strength, and the transforms ftmx/potmx [nbin][nq]
+    on the reference's float grids rr=(i+.5F)dr (grsq.cpp:53), qq=(i+.5F)dq (grsq.cpp:272)."""
+    sqex = np.atleast_2d(np.asarray(sqex, np.float64))
+    wt = np.atleast_2d(np.asarray(wt, np.float64)) * strength
+    ff = np.asarray(ff, np.float64).reshape(sqex.shape[0], nq, ntype)
+    cnt = np.bincount(np.asarray(typ), minlength=ntype).astype(np.float64)
+    natom = cnt.sum()
+    P = ntype * (ntype + 1) // 2
+    nsq = sqex.shape[0]
+    sqwt = np.zeros((nsq, P, nq)); fwt = np.zeros((nsq, P, nq))
+    for n in range(nsq):
+        cifi2 = (ff[n] @ cnt / natom) ** 2                       # grsq.cpp:993-997
+        ip = 0
+        for j in range(ntype):
+            ni = cnt[j] / natom ** 2
+            for k in range(j, ntype):
+                fw = ff[n, :, j] * ff[n, :, k] / cifi2
+                sqwt[n, ip] = fw * cnt[k] * ni * (1 if k == j else 2)   # grsq.cpp:1003-1006
+                fwt[n, ip] = fw * wt[n]
+                ip += 1
+    dq = np.float32(np.float32(qmax) / np.float32(nq))
+    qq = ((np.arange(nq, dtype=np.float32) + np.float32(0.5)) * dq).astype(np.float64)
+    rr = ((np.arange(nbin, dtype=np.float32) + np.float32(0.5)) * np.float32(dr)).astype(np.float64)
+    qr = rr[:, None] * qq[None, :]
+    j0 = np.sin(qr) / qr
+    return dict(sqwt=sqwt, fwt=fwt, sqex=sqex, wt=wt, potmx=j0, ftmx=(j0 - np.cos(qr)) / rr[:, None] ** 2,
+                natom=natom, P=P, nsq=nsq)
+
+
+def rmdf_update(st, sq_partial, deltasq, gamma):
+    """compute_Qspace (grsq.cpp:1061-1118): returns erg_exp, new deltasq [n][nq], force_q [P][nq], S_n."""
+    sq_partial = np.asarray(sq_partial, np.float64)
+    sqn = np.einsum("pq,npq->nq", sq_partial, st["sqwt"])
+    d = sqn - st["sqex"]
+    erg = float((d * d * st["wt"]).sum()) * st["natom"] * 0.25
+    dsq = deltasq + gamma * (d - deltasq)
+    fq = np.einsum("nq,npq->pq", dsq, st["fwt"])
+    return erg, dsq, fq, sqn
+
+
+def rmdf_tables(st, fq, Fbase, Ubase, potential=True):
+    """compute_Rspace / compute_Potential (grsq.cpp:1120-1210): base + force_q x transform."""
+    F = np.array(Fbase, np.float64); U = np.array(Ubase, np.float64)
+    nbin = st["ftmx"].shape[0]
+    F[:, :nbin] += fq @ st["ftmx"].T
+    if potential:
+        U[:, :nbin] += fq @ st["potmx"].T
+    return F, U

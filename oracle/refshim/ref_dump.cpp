@@ -13,7 +13,10 @@
 //  * initial velocities can be read from a file instead of ENVIRON::initV;
 //  * per-thread energy/virial/KE partial sums are added in thread order after a barrier rather
 //    than in a `critical` section, so that repeated runs are bit-identical;
-//  * the thermostat can be switched off (scale_interval 0) for NVE parity runs.
+//  * the thermostat can be switched off (scale_interval 0) for NVE parity runs;
+//  * g(r) steps (gr.tally, reduce_local, SQ::compute, RMDF::compute_Qspace/Rspace/Potential,
+//    run.cpp:286-299) run only when `gr_interval` is given, and RMDF only with an `rmdf` line
+//    (run.cpp always constructs RMDF and needs at least one target file for it).
 #include <omp.h>
 
 #include <algorithm>
@@ -47,6 +50,9 @@ struct Cfg {
   unsigned seed = 12345;
   bool lj = true;
   std::vector<std::vector<float>> bond, angle, dih;
+  std::vector<std::string> rmdf_files;
+  float rmdf_strength = 0, rmdf_gamma = 1;
+  int gr_interval = 0, gr_interval_long = 0;
 };
 
 void die(const char* m) { fprintf(stderr, "ref_dump: %s\n", m); exit(2); }
@@ -69,6 +75,15 @@ Cfg parse(const char* path) {
     else if (k == "table") { sscanf(line, "%*s %d %511s", &c.nbin, s1); c.table = s1; }
     else if (k == "nnp") { sscanf(line, "%*s %f %d %511s %511s", &c.nnp_cutoff, &c.nnp_nbin, s1, s2); c.nnp_param = s1; c.nnp_wt = s2; }
     else if (k == "no_lj") c.lj = false;
+    else if (k == "rmdf") {
+      char f1[512] = "", f2[512] = "";
+      int n = sscanf(line, "%*s %f %f %511s %511s", &c.rmdf_strength, &c.rmdf_gamma, f1, f2);
+      if (n < 3) die("bad rmdf line");
+      c.rmdf_files.push_back(f1);
+      if (n == 4) c.rmdf_files.push_back(f2);
+    } else if (k == "gr_interval") {
+      if (sscanf(line, "%*s %d %d", &c.gr_interval, &c.gr_interval_long) != 2) die("bad gr_interval line");
+    }
     else if (k == "cutoff") fl(c.cutoff);
     else if (k == "skin") fl(c.skin);
     else if (k == "gr_cutoff") fl(c.gr_cutoff);
@@ -162,6 +177,12 @@ int main(int argc, char** argv) {
   }
   GR gr(c.lj ? c.nbin : c.nnp_nbin, c.gr_cutoff, list_cut);
   SQ sq(c.nq, c.qmax, &gr);
+  RMDF* rmdf = nullptr;
+  if (!c.rmdf_files.empty()) {
+    std::vector<char*> names;
+    for (auto& f : c.rmdf_files) names.push_back(const_cast<char*>(f.c_str()));
+    rmdf = new RMDF((int)names.size(), names.data(), &sq, c.rmdf_strength, c.rmdf_gamma, pair, pair ? nullptr : nnp);
+  }
 
   if (!c.vel.empty()) {
     FILE* fp = fopen(c.vel.c_str(), "rb");
@@ -176,7 +197,8 @@ int main(int argc, char** argv) {
   }
 
   const int NT = ENVIRON::NUM_THREAD;
-  std::vector<double> erg_t(NT), vir_t(NT), ke_t(NT), enn_t(NT);
+  std::vector<double> erg_t(NT), vir_t(NT), ke_t(NT), enn_t(NT), exp_t(NT, 0.0);
+  std::vector<double> log_exp;
   std::vector<int> valid_t(NT);
   std::vector<double> log_e, log_w, log_k, log_enn;
   std::vector<int> log_build;
@@ -278,6 +300,28 @@ int main(int argc, char** argv) {
           dump(c, "qq.f32", sq.qq, (size_t)sq.nbin_q);
           dump(c, "rr.f32", gr.rr, (size_t)gr.nbin_r);
         }
+        if (rmdf) {
+          // one refinement update on this S(q): compute_Qspace, compute_Rspace, compute_Potential
+          exp_t[me] = rmdf->compute_Qspace(me);
+#pragma omp barrier
+          if (pair) { rmdf->compute_Rspace(me); rmdf->compute_Potential(me); }
+          else { rmdf->compute_Rspace_NNP(me); rmdf->compute_Potential_NNP(me); }
+#pragma omp barrier
+#pragma omp single
+          {
+            double e = 0;
+            for (int t = 0; t < NT; ++t) e += exp_t[t];
+            dump(c, "rmdf_erg.f64", &e, 1);
+            dump(c, "rmdf_sq.f32", rmdf->sq[0], (size_t)c.rmdf_files.size() * sq.nbin_q);
+            if (pair) {
+              dump(c, "tbl_force.f32", pair->force[0], (size_t)ENVIRON::npair * (pair->nbin_r + 1));
+              dump(c, "tbl_pot.f32", pair->potential[0], (size_t)ENVIRON::npair * (pair->nbin_r + 1));
+            } else {
+              dump(c, "tbl_force.f32", nnp->tbl_f_pair[0][0], (size_t)ENVIRON::npair * 4 * (nnp->nbin_r + 1));
+              dump(c, "tbl_pot.f32", nnp->tbl_pair[0][0], (size_t)ENVIRON::npair * 4 * (nnp->nbin_r + 1));
+            }
+          }
+        }
         gr.tally<true>(&list_pair);
 #pragma omp barrier
 #pragma omp single
@@ -287,6 +331,27 @@ int main(int argc, char** argv) {
             for (int p = 0; p < ENVIRON::npair; ++p)
               for (int k = 0; k < gr.nbin_r_inner; ++k) cnt[(size_t)p * gr.nbin_r_inner + k] += gr.gr_local[t][p][k];
           dump(c, "gr_inner_counts.i64", cnt.data(), cnt.size());
+        }
+      }
+
+      // g(r) step: tally, reduce, S(q), RMDF (run.cpp:286-299)
+      if (!snapshot && c.gr_interval > 0 && !(md_step % c.gr_interval)) {
+#pragma omp barrier
+        if (md_step % c.gr_interval_long) gr.tally<true>(&list_pair);
+        else gr.tally(bin_list_gr, &local);
+#pragma omp barrier
+        gr.reduce_local(me);
+#pragma omp barrier
+        sq.compute(me);
+        if (rmdf) exp_t[me] = rmdf->compute_Qspace(me);
+#pragma omp barrier
+        if (rmdf) {
+          if (pair) rmdf->compute_Rspace(me);
+          else rmdf->compute_Rspace_NNP(me);
+          if (f_log && c.rmdf_gamma != 1) {
+            if (pair) rmdf->compute_Potential(me);
+            else rmdf->compute_Potential_NNP(me);
+          }
         }
       }
 
@@ -367,6 +432,9 @@ int main(int argc, char** argv) {
           erg = e + (nnp ? enn : 0); vir = w; ekin = k;
           log_e.push_back(erg); log_w.push_back(vir); log_k.push_back(ekin);
           log_enn.push_back(nnp ? enn : 0);
+          float ex = 0;
+          for (int t = 0; t < NT; ++t) ex += (float)exp_t[t];
+          log_exp.push_back(ex);
           log_build.push_back((int)list_pair.nbuild);
         }
       }
@@ -382,6 +450,14 @@ int main(int argc, char** argv) {
   dump(c, "log_w.f64", log_w.data(), log_w.size());
   dump(c, "log_k.f64", log_k.data(), log_k.size());
   dump(c, "log_enn.f64", log_enn.data(), log_enn.size());
+  dump(c, "log_exp.f64", log_exp.data(), log_exp.size());
+  if (rmdf && !snapshot) {
+    if (pair) {
+      dump(c, "tbl_force.f32", pair->force[0], (size_t)ENVIRON::npair * (pair->nbin_r + 1));
+      dump(c, "tbl_pot.f32", pair->potential[0], (size_t)ENVIRON::npair * (pair->nbin_r + 1));
+    }
+    dump(c, "rmdf_sq.f32", rmdf->sq[0], (size_t)c.rmdf_files.size() * sq.nbin_q);
+  }
   FILE* fp = fopen((c.out + "/info.txt").c_str(), "w");
   fprintf(fp, "natom %d\nnghost %d\nntot %d\nnum_gx %d\nnpair %d\nnbin_r %d\nnbin_r_inner %d\nnbin_q %d\n"
           "full_pairs %lld\nnbuild_last %d\nt_loop %.9f\nsteps %d\nthreads %d\n",

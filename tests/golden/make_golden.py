@@ -14,6 +14,11 @@ is run on the seeded cases of tests/cases.py; its outputs are stored compactly:
                  network energy, forces (bonded + NNP).
 * mixture2000.npz  2000-atom two-species LJ+Coulomb liquid at 0.035 A^-3: g(r) counts to 15 A in
                  0.01 A bins, the reference's float g(r) and S(q) on 512 q points, forces.
+* rmdf2000.npz   the same liquid with RMDF (grsq.cpp:899-1377) against a seeded synthetic S(q)
+                 target (strength 0.02, gamma 0.5): the refined force/potential tables, weighted
+                 S(q) and penalty of one update on the snapshot's S(q); and a 20-step NVE run with
+                 g(r) steps every 5 steps (cell-based every 10): per-log-step penalty, final x, v
+                 and tables.
 
 Run:  python tests/golden/make_golden.py   (needs /root/reference/src and `make -C oracle ref`).
 """
@@ -74,6 +79,36 @@ def mixture2000(work):
     print("mixture2000:", s.natom, "atoms, gr bins", out["gr_counts"].shape)
 
 
+RMDF_STRENGTH, RMDF_GAMMA = 0.02, 0.5
+
+
+def rmdf_target(work, ntype=2):
+    from nnpengine_b200 import systems as S
+    q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, ntype, seed=7)
+    path = os.path.join(work, "sq_target.txt")
+    S.write_sq_target(path, q, sqex, wt, ff)
+    return path, (q, sqex, wt, ff)
+
+
+def rmdf2000(work):
+    s, table = cases.mixture_case()
+    f = cases.write_inputs(s, table, work)
+    v0 = os.path.join(work, "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    tpath, (q, sqex, wt, ff) = rmdf_target(work)
+    base = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 15, "nq": 512,
+            "qmax": 20, "rmdf": f"{RMDF_STRENGTH} {RMDF_GAMMA} {tpath}"}
+    snap = orc.run_ref_dump({**base, "velocity": v0, "mode": "snapshot"}, os.path.join(work, "snap"))
+    md = orc.run_ref_dump({**base, "velocity": f["vel"], "mode": "md", "steps": 20, "dt": 1, "log_interval": 5,
+                           "gr_interval": "5 10"}, os.path.join(work, "md"))
+    out = dict(sqex=sqex, wt=wt, ff=ff, q=q, tbl_force=snap["tbl_force"].reshape(3, -1), tbl_pot=snap["tbl_pot"].reshape(3, -1),
+               rmdf_sq=snap["rmdf_sq"], rmdf_erg=snap["rmdf_erg"], sq_f32=snap["sq"].reshape(3, -1),
+               md_x=md["x"].reshape(-1, 3), md_v=md["v"].reshape(-1, 3), md_erg=md["log_e"], md_exp=md["log_exp"],
+               md_tbl_force=md["tbl_force"].reshape(3, -1), md_tbl_pot=md["tbl_pot"].reshape(3, -1))
+    np.savez_compressed(os.path.join(HERE, "rmdf2000.npz"), **out)
+    print("rmdf2000: penalty", float(snap["rmdf_erg"][0]), "md penalties", md["log_exp"])
+
+
 def nnp_gauss648(work):
     from nnpengine_b200 import nnp_model as NM
     s, table = cases.water_case()
@@ -97,3 +132,4 @@ if __name__ == "__main__":
         water648(os.path.join(t, "w"))
         mixture2000(os.path.join(t, "m"))
         nnp_gauss648(os.path.join(t, "n"))
+        rmdf2000(os.path.join(t, "r"))

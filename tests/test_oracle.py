@@ -139,3 +139,24 @@ def test_embedding_nnp_forces_are_energy_gradient():
             step = float(xp[atom, d]) - float(xm[atom, d])
             grad = (run(xp)["e_net"] - run(xm)["e_net"]) / step
             assert abs(grad + f[atom, d]) < 2e-4 * np.abs(f[atom]).max() + 1e-6, (atom, d, grad, f[atom, d])
+
+
+def test_restated_rmdf_matches_reference():
+    """The FP64 RMDF restatement on the reference's own float S(q) reproduces the reference's
+    refined tables to within its float accumulation (512 terms added to the base value)."""
+    g = np.load(os.path.join(cases.GOLDEN, "rmdf2000.npz"))
+    s, table = cases.mixture_case()
+    F, U = cases.table_as_loaded(table[1], table[2])
+    st = orc.rmdf_setup(s.typ, 2, 1000, np.float32(10) / np.float32(1000), 512, 20.0, g["sqex"][None], g["wt"][None],
+                        g["ff"][None], 0.02)
+    erg, dsq, fq, sqn = orc.rmdf_update(st, g["sq_f32"], np.zeros((1, 512)), 0.5)
+    Fo, Uo = orc.rmdf_tables(st, fq, F, U)
+    assert abs(erg - g["rmdf_erg"][0]) < 1e-6 * abs(g["rmdf_erg"][0])
+    np.testing.assert_allclose(sqn[0], g["rmdf_sq"], rtol=1e-5, atol=1e-6 * np.abs(sqn).max())
+    for o, r in ((Fo, g["tbl_force"]), (Uo, g["tbl_pot"])):
+        u = np.spacing(np.maximum(np.abs(o), np.abs(r)).astype(np.float32)).astype(np.float64)
+        assert (np.abs(o - r) / u).max() <= 1024
+    # the target file round-trips through the reference's reader format
+    from nnpengine_b200 import systems as S
+    q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, 2, seed=7)
+    np.testing.assert_array_equal(sqex, g["sqex"])
