@@ -60,6 +60,8 @@ void nnpe_destroy(nnpe_ctx* ctx);
 const char* nnpe_last_error(const nnpe_ctx* ctx);
 /* Raw device error bits since the last call to this function (then cleared). */
 int nnpe_device_errors(nnpe_ctx* ctx, int* bits);
+/* Device memory this context holds (bytes of its own allocations). */
+int nnpe_device_bytes(const nnpe_ctx* ctx, int64_t* bytes);
 /* Stream all work of this context is issued on (cudaStream_t as void*). */
 void* nnpe_stream(nnpe_ctx* ctx);
 
@@ -248,6 +250,102 @@ int nnpe_rmdf_step(nnpe_ctx* ctx, int potential, double* erg_exp);
 int nnpe_rmdf_get(nnpe_ctx* ctx, double* sq, double* deltasq, double* force_q);
 /* RMDF::dumpSQ (grsq.cpp:1380-1416). */
 int nnpe_rmdf_dump_sq(nnpe_ctx* ctx, const char* fname, int append);
+
+/* ---- serving: a stream of independent MD replicas on one GPU ------------------------------
+ * No counterpart in the reference, which holds one system per process (ENVIRON is a static
+ * singleton, environ.h:20-123) and so runs such a stream as one run after another. A server owns a
+ * worker thread that admits queued requests in arrival order as soon as a replica slot is free and
+ * the request's device footprint fits the HBM budget, keeps a CUDA-graph launch of chunk_steps MD
+ * steps in flight on every resident replica (replicas of different sizes overlap on the device; new
+ * arrivals join while others run), and retires finished replicas. Each replica is a context as
+ * above; its result does not depend on what else runs. */
+typedef struct nnpe_server nnpe_server;
+
+/* Force field and run settings shared by all replicas; arrays are copied by nnpe_server_create.
+ * The pair table, bonded coefficients (stored forms) and network follow nnpe_pair_set_table,
+ * nnpe_bonded_set and nnpe_nnp_set; force == NULL: no pair term; nnp_kind < 0: no network. */
+typedef struct nnpe_serve_config {
+  int device;
+  int max_replicas;          /* resident replicas at most */
+  int64_t hbm_budget;        /* device bytes the resident replicas may hold */
+  int chunk_steps;           /* MD steps per launch; also the thermostat and log interval */
+  double pair_cutoff, skin;
+  int neigh_cap;
+  double dt;
+  int fp64_state;
+  int thermostat;            /* 0 NVE, 1 Andersen (run.cpp:360-364) at the request's temperature */
+  double thermo_frac;
+  int ntype;
+  int nbin;
+  const float* force;        /* [npair][nbin+1] F(r)/r */
+  const float* potential;    /* [npair][nbin+1] U(r) */
+  int nbtyp;
+  const float* bcoef;
+  int natyp;
+  const float* acoef;
+  int ndtyp;
+  const float* dcoef;
+  int nnp_kind;
+  double nnp_cutoff;
+  int nnp_nbin;
+  double nnp_scale;
+  int e1, e2, h1, h2;
+  const float *coef_p, *coef_w, *coef_d, *coef_r, *embw, *fitw;
+  int nnp_bf16;
+} nnpe_serve_config;
+
+/* One MD request: a system in the arrays of nnpe_set_system, initial velocities, bonded terms in
+ * the form of nnpe_bonded_set, and nsteps MD steps (md_step 0..nsteps-1) at `temperature`
+ * (Andersen when the server's thermostat is on; seed keys its random numbers). */
+typedef struct nnpe_request {
+  int natom;
+  double bl;
+  const int* typ;
+  const float* mass;
+  const float* q;
+  const float* x;
+  const float* v;
+  const int* mol_id;
+  const int* intra_id;
+  const int* atom_moltype;
+  int nmoltype, nmax;
+  const int* special;
+  int nbond;
+  const int* bonds;
+  int nangle;
+  const int* angles;
+  int ndih;
+  const int* dihs;
+  int nsteps;
+  double temperature;
+  uint64_t seed;
+} nnpe_request;
+
+typedef struct nnpe_request_stats {
+  int64_t id;
+  int natom, nsteps;
+  int status;                    /* 0 queued, 1 resident, 2 done, < 0: failed with NNPE_E* code -status */
+  double t_submit, t_admit, t_done;   /* seconds since the server was created */
+  int64_t bytes;                 /* device bytes the replica held */
+  double erg, ekin, temperature; /* last log record (first step of the last chunk) */
+} nnpe_request_stats;
+
+int nnpe_server_create(const nnpe_serve_config* cfg, nnpe_server** out);
+/* Queues a copy of the request; returns at once with its id. */
+int nnpe_server_submit(nnpe_server* srv, const nnpe_request* req, int64_t* id);
+/* Blocks until request id is done (timeout_s < 0: no limit; NNPE_ETIMEOUT when it expires). */
+int nnpe_server_wait(nnpe_server* srv, int64_t id, double timeout_s, nnpe_request_stats* st);
+/* Final positions and velocities (atom-id order, float [natom*3]) of a finished request. */
+int nnpe_server_result(nnpe_server* srv, int64_t id, float* x, float* v, nnpe_request_stats* st);
+/* Blocks until every submitted request is done. */
+int nnpe_server_drain(nnpe_server* srv, double timeout_s);
+int nnpe_server_info(nnpe_server* srv, int64_t* done, int64_t* queued, int* resident, int64_t* bytes_in_use,
+                     int64_t* peak_bytes, int* peak_resident);
+/* Device bytes the admission test reserves for a request of natom atoms in a box of edge bl. */
+int64_t nnpe_server_footprint(nnpe_server* srv, int natom, double bl);
+const char* nnpe_server_error(nnpe_server* srv);
+/* Stops the worker after the chunks in flight and frees every replica. */
+void nnpe_server_destroy(nnpe_server* srv);
 
 #ifdef __cplusplus
 }

@@ -32,6 +32,7 @@ _SIGS = {
     "nnpe_last_error": (C.c_char_p, [_vp]),
     "nnpe_device_errors": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "nnpe_stream": (_vp, [_vp]),
+    "nnpe_device_bytes": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "nnpe_set_system": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _i32p, _f32p, _f32p, _f32p, _i32p, _i32p, _i32p,
                                   C.c_int, C.c_int, _i32p]),
     "nnpe_load_system_file": (C.c_int, [_vp, C.c_char_p]),

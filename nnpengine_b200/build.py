@@ -28,6 +28,7 @@ UNITS = {
     "integrate.cu": EXACT,
     "gr.cu": EXACT,
     "rmdf.cu": EXACT,
+    "serve.cu": [],
     "nnp.cu": [],
     "nnp_tc.cu": [],
 }

@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -21,16 +23,42 @@ int nnpe_sm_count(int device) {
   return n > 0 ? n : 148;
 }
 
+static std::mutex g_alloc_mu;
+static std::unordered_map<void*, std::pair<nnpe_ctx*, size_t>> g_allocs;
+
+cudaError_t dev_malloc(nnpe_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    g_allocs[*p] = {c, bytes};
+    c->dev_bytes += (int64_t)bytes;
+  }
+  return e;
+}
+
+void dev_free(void* p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    auto it = g_allocs.find(p);
+    if (it != g_allocs.end()) {
+      it->second.first->dev_bytes -= (int64_t)it->second.second;
+      g_allocs.erase(it);
+    }
+  }
+  cudaFree(p);
+}
+
 template <typename T>
 static int dalloc(nnpe_ctx* c, T** p, size_t n) {
-  if (*p) { cudaFree(*p); *p = nullptr; }
+  if (*p) { dev_free(*p); *p = nullptr; }
   if (n == 0) n = 1;
-  NNPE_CUDA(c, cudaMalloc((void**)p, n * sizeof(T)));
+  NNPE_CUDA(c, dev_malloc(c, (void**)p, n * sizeof(T)));
   return 0;
 }
 template <typename T>
 static void dfree(T** p) {
-  if (*p) cudaFree(*p);
+  if (*p) dev_free(*p);
   *p = nullptr;
 }
 #define TRY(x) do { int rc_ = (x); if (rc_) return rc_; } while (0)
@@ -45,9 +73,9 @@ int nnpe_create(int device, nnpe_ctx** out) {
   auto* c = new nnpe_ctx();
   c->device = device;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return NNPE_ECUDA; }
-  if (cudaMalloc(&c->d_ctrl, sizeof(int) * CTRL_WORDS) != cudaSuccess ||
+  if (dev_malloc(c, (void**)&c->d_ctrl, sizeof(int) * CTRL_WORDS) != cudaSuccess ||
       cudaMallocHost(&c->h_ctrl, sizeof(int) * CTRL_WORDS) != cudaSuccess ||
-      cudaMalloc(&c->d_red, sizeof(double) * 16) != cudaSuccess ||
+      dev_malloc(c, (void**)&c->d_red, sizeof(double) * 16) != cudaSuccess ||
       cudaMallocHost(&c->h_red, sizeof(double) * 16) != cudaSuccess) {
     delete c;
     return NNPE_ECUDA;
@@ -98,6 +126,13 @@ void nnpe_destroy(nnpe_ctx* c) {
 }
 
 const char* nnpe_last_error(const nnpe_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int nnpe_device_bytes(const nnpe_ctx* c, int64_t* bytes) {
+  if (!c || !bytes) return NNPE_EARG;
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  *bytes = c->dev_bytes;
+  return NNPE_OK;
+}
 void* nnpe_stream(nnpe_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int nnpe_natom(const nnpe_ctx* c) { return c ? c->natom : 0; }
 int nnpe_npair(const nnpe_ctx* c) { return c ? c->npair : 0; }

@@ -459,8 +459,8 @@ extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, 
   cudaSetDevice(c->device);
   const int N = c->natom;
   if (!c->d_xstage) {
-    NNPE_CUDA(c, cudaMalloc(&c->d_xstage, sizeof(float) * 3 * N));
-    NNPE_CUDA(c, cudaMalloc(&c->d_fstage, sizeof(float) * 3 * N));
+    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_xstage, sizeof(float) * 3 * N));
+    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_fstage, sizeof(float) * 3 * N));
   }
   if (!c->first_step_done && !c->force_step_init) {
     k_qm_to_pos<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_qm, c->d_pos, N);

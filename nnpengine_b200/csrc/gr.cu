@@ -112,15 +112,15 @@ __global__ void k_sq(const double* __restrict__ gr, double* __restrict__ sq, dou
 }  // namespace
 
 static int dalloc_u64(nnpe_ctx* c, unsigned long long** p, size_t n) {
-  if (*p) cudaFree(*p);
+  if (*p) dev_free(*p);
   *p = nullptr;
-  NNPE_CUDA(c, cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(unsigned long long)));
+  NNPE_CUDA(c, dev_malloc(c, (void**)p, std::max<size_t>(n, 1) * sizeof(unsigned long long)));
   return 0;
 }
 static int dalloc_f64(nnpe_ctx* c, double** p, size_t n) {
-  if (*p) cudaFree(*p);
+  if (*p) dev_free(*p);
   *p = nullptr;
-  NNPE_CUDA(c, cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(double)));
+  NNPE_CUDA(c, dev_malloc(c, (void**)p, std::max<size_t>(n, 1) * sizeof(double)));
   return 0;
 }
 

@@ -229,9 +229,9 @@ static int prepare_run(nnpe_ctx* c, int max_log) {
   if (!c->d_table && !c->nnp && c->pair_on) return nnpe_fail(c, NNPE_EARG, "nnpe_run: no pair table");
   cudaSetDevice(c->device);
   if (max_log > c->log_cap) {
-    if (c->d_log) cudaFree(c->d_log);
+    if (c->d_log) dev_free(c->d_log);
     c->d_log = nullptr;
-    NNPE_CUDA(c, cudaMalloc(&c->d_log, sizeof(LogRec) * max_log));
+    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_log, sizeof(LogRec) * max_log));
     c->log_cap = max_log;
     for (auto& g : c->graph_exec)
       if (g) { cudaGraphExecDestroy(g); g = nullptr; }
@@ -281,6 +281,33 @@ extern "C" int nnpe_run(nnpe_ctx* c, int nsteps, int log_interval, nnpe_thermo* 
     if (int rc = enqueue_step(c, step_variant(c, step0 + s, log_interval))) return rc;
   return finish_run(c, log, max_log, nlog);
 }
+
+// Launch steps step0..step0+nsteps-1 from the per-variant step graphs without waiting for them
+// (the serving loop tracks md_step on the host, so nothing is read back here).
+int run_graph_launch(nnpe_ctx* c, int step0, int nsteps, int log_interval) {
+  if (!c->graph_valid) {
+    for (auto& g : c->graph_exec)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->graph_valid = true;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int v = step_variant(c, step0 + s, log_interval);
+    if (!c->graph_exec[v]) {
+      cudaGraph_t g;
+      NNPE_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_step(c, v);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return nnpe_fail(c, NNPE_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      NNPE_CUDA(c, cudaGraphInstantiate(&c->graph_exec[v], g, 0));
+      cudaGraphDestroy(g);
+    }
+    NNPE_CUDA(c, cudaGraphLaunch(c->graph_exec[v], c->stream));
+  }
+  return 0;
+}
+int run_prepare(nnpe_ctx* c, int max_log) { return prepare_run(c, max_log); }
+int run_finish(nnpe_ctx* c, nnpe_thermo* log, int max_log, int* nlog) { return finish_run(c, log, max_log, nlog); }
 
 extern "C" int nnpe_run_graph(nnpe_ctx* c, int nsteps, int log_interval, nnpe_thermo* log, int max_log, int* nlog) {
   if (int rc = prepare_run(c, max_log)) return rc;

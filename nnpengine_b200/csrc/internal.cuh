@@ -145,6 +145,8 @@ struct nnpe_ctx {
   NnpModel* nnp = nullptr;
   // RMDF refinement of the pair table (d_red[4] holds the last erg_exp)
   RmdfState* rmdf = nullptr;
+  // device bytes held by this context (dev_malloc / dev_free)
+  int64_t dev_bytes = 0;
   // CUDA graphs of the step variants
   cudaGraphExec_t graph_exec[16] = {};
   bool graph_valid = false;
@@ -217,4 +219,8 @@ int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
 int nnp_forces_enqueue(nnpe_ctx* c, bool ev);
 int nnpe_bonded_coefs(nnpe_ctx* c, const float* bcoef, const float* acoef, const float* dcoef);
 void nnp_free(nnpe_ctx* c);
+// Device allocations of a context go through these two, which keep the context's byte count
+// (nnpe_ctx::dev_bytes) for the serving loop's memory ledger.
+cudaError_t dev_malloc(nnpe_ctx* c, void** p, size_t bytes);
+void dev_free(void* p);
 void rmdf_free(nnpe_ctx* c);

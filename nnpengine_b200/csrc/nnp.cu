@@ -30,14 +30,14 @@
 // ---------------------------------------------------------------------------------------------
 template <typename T>
 static int nalloc(nnpe_ctx* c, T** p, size_t n) {
-  if (*p) cudaFree(*p);
+  if (*p) dev_free(*p);
   *p = nullptr;
-  NNPE_CUDA(c, cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)));
+  NNPE_CUDA(c, dev_malloc(c, (void**)p, std::max<size_t>(n, 1) * sizeof(T)));
   return 0;
 }
 template <typename T>
 static void nfree(T** p) {
-  if (*p) cudaFree(*p);
+  if (*p) dev_free(*p);
   *p = nullptr;
 }
 

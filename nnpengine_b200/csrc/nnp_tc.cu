@@ -657,7 +657,7 @@ void nnp_tc_free(NnpModel* m) {
   if (!t) return;
   for (void* p : {(void*)t->d_wdesc, (void*)t->d_facc, (void*)t->d_fit, (void*)t->d_emb_small, (void*)t->d_fit_small,
                   (void*)t->d_tile_sp, (void*)t->d_tile_row, (void*)t->d_soff})
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
   delete t;
   m->tc = nullptr;
 }
@@ -711,12 +711,12 @@ int nnp_tc_setup(nnpe_ctx* c) {
   t->ntiles = (int)tsp.size();
   t->fit_stride = stride_el * 2;
   auto up = [&](void** d, const void* h, size_t bytes) -> int {
-    NNPE_CUDA(c, cudaMalloc(d, std::max<size_t>(bytes, 16)));
+    NNPE_CUDA(c, dev_malloc(c, d, std::max<size_t>(bytes, 16)));
     if (bytes) NNPE_CUDA(c, cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
     return 0;
   };
   if (int rc = up((void**)&t->d_wdesc, wdesc.data(), wdesc.size() * 2)) return rc;
-  NNPE_CUDA(c, cudaMalloc((void**)&t->d_facc, sizeof(unsigned long long) * 3 * std::max(c->natom, 1)));
+  NNPE_CUDA(c, dev_malloc(c, (void**)&t->d_facc, sizeof(unsigned long long) * 3 * std::max(c->natom, 1)));
   if (int rc = up((void**)&t->d_fit, fit.data(), fit.size() * 2)) return rc;
   if (int rc = up((void**)&t->d_emb_small, emb_small.data(), emb_small.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_fit_small, fit_small.data(), fit_small.size() * 4)) return rc;

@@ -113,9 +113,9 @@ __global__ void k_rmdf_r(const double* __restrict__ fq, const double* __restrict
 
 template <typename T>
 int dput(nnpe_ctx* c, T** d, const std::vector<T>& h) {
-  if (*d) cudaFree(*d);
+  if (*d) dev_free(*d);
   *d = nullptr;
-  NNPE_CUDA(c, cudaMalloc((void**)d, sizeof(T) * std::max<size_t>(h.size(), 1)));
+  NNPE_CUDA(c, dev_malloc(c, (void**)d, sizeof(T) * std::max<size_t>(h.size(), 1)));
   if (!h.empty()) NNPE_CUDA(c, cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
   return 0;
 }
@@ -129,7 +129,7 @@ void rmdf_free(nnpe_ctx* c) {
   if (!r) return;
   for (void* p : {(void*)r->d_sqwt, (void*)r->d_fwt, (void*)r->d_sqex, (void*)r->d_wt, (void*)r->d_dsq, (void*)r->d_sqn,
                   (void*)r->d_fq, (void*)r->d_ftmx, (void*)r->d_potmx, (void*)r->d_base})
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
   delete r;
   c->rmdf = nullptr;
 }
@@ -228,7 +228,7 @@ extern "C" int nnpe_rmdf_set(nnpe_ctx* c, int n_sq, const double* sqex, const do
   if (int rc = dput(c, &r->d_potmx, potmx)) return rc;
   // the *_base tables: the table as it stands now (loadPotential(1) copies base to force, pair.cpp:245-250)
   const size_t tsz = nnp ? (size_t)P * 4 * (nbin + 1) : (size_t)P * (nbin + 1);
-  NNPE_CUDA(c, cudaMalloc((void**)&r->d_base, sizeof(float2) * tsz));
+  NNPE_CUDA(c, dev_malloc(c, (void**)&r->d_base, sizeof(float2) * tsz));
   NNPE_CUDA(c, cudaMemcpy(r->d_base, rmdf_table(c), sizeof(float2) * tsz, cudaMemcpyDeviceToDevice));
   double zero5 = 0;
   NNPE_CUDA(c, cudaMemcpy(c->d_red + 4, &zero5, sizeof(double), cudaMemcpyHostToDevice));

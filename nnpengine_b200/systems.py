@@ -315,3 +315,33 @@ def synthetic_sq_target(nq: int = 512, qmax: float = 20.0, ntype: int = 2, q_min
     wt = (q >= q_min).astype(np.float32)
     ff = np.tile(np.linspace(1.0, 0.6, ntype, dtype=np.float32), (nq, 1))
     return q, sqex, wt, ff
+
+
+WATER_MOLAR_MASS = 18.01528   # g/mol
+AVOGADRO_A3 = 0.602214076     # N_A * 1e-24 (g/cm^3 -> g/mol per A^3)
+
+
+def water_request_box(natom: int, density: float, seed: int, temperature: float) -> System:
+    """Water box of about `natom` atoms (rounded down to whole molecules, at least one) at `density`
+    g/cm^3: the cubic box holding that many molecules, molecules on the smallest cubic lattice that
+    fits them (a seeded subset of its sites), Maxwell-Boltzmann velocities at `temperature`."""
+    nmol = max(1, natom // 3)
+    bl = (nmol * WATER_MOLAR_MASS / (density * AVOGADRO_A3)) ** (1.0 / 3.0)
+    n_side = int(math.ceil(nmol ** (1.0 / 3.0) - 1e-9))
+    return water_box(n_side, bl, seed=seed, temperature=temperature, nmol=nmol)
+
+
+def serving_trace(nreq: int = 256, seed: int = 3, natom_range=(300, 30000), density_range=(0.95, 1.05),
+                  temp_range=(250.0, 400.0), steps_range=(100, 5000), rate: float = 20.0):
+    """Seeded request stream of the served-replica workload: atom counts log-uniform in natom_range,
+    densities and temperatures uniform, step counts uniform integers, Poisson arrivals at `rate`
+    per second. Returns a list of dicts (arrival time in s, natom, density, temperature, nsteps, seed)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(natom_range[0]), np.log(natom_range[1])
+    natom = np.exp(rng.uniform(lo, hi, nreq)).astype(int)
+    dens = rng.uniform(*density_range, nreq)
+    temp = rng.uniform(*temp_range, nreq)
+    steps = rng.integers(steps_range[0], steps_range[1] + 1, nreq)
+    arrive = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    return [dict(t=float(arrive[k]), natom=int(natom[k]), density=float(dens[k]), temperature=float(temp[k]),
+                 nsteps=int(steps[k]), seed=int(1000 + k)) for k in range(nreq)]

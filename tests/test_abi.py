@@ -45,3 +45,33 @@ def test_water_files_roundtrip(tmp_path):
     np.testing.assert_array_equal(x, s.x)
     mol = open(str(p).replace("init.txt", "init.mol0")).read()
     assert "3 atoms" in mol and "Bonds" in mol and "Angles" in mol
+
+
+def test_serving_struct_layout_matches_header(tmp_path):
+    """The ctypes mirrors of nnpe_serve_config / nnpe_request / nnpe_request_stats have the C
+    header's sizes and field offsets (compiled here with gcc against include/nnpe.h)."""
+    import os
+    import shutil
+    import subprocess
+    from nnpengine_b200 import serve
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    inc = os.path.join(os.path.dirname(_lib.__file__), "..", "include")
+    structs = {"nnpe_serve_config": serve.ServeConfig, "nnpe_request": serve.Request,
+               "nnpe_request_stats": serve.RequestStats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "nnpe.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
