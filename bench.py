@@ -43,6 +43,11 @@ WORKLOADS = {
     "water3k-classical": dict(n_side=10, bl=31.04, nmol=None, nnp=None,
                               desc="3,000-atom water (1,000 molecules, 31.04 A box), tabulated LJ + DSF Coulomb at 10 A, "
                                    "2 A skin, bonds + angles, dt 0.5 fs NVE"),
+    "serve256": dict(serve=True, nnp="bf16",
+                     desc="served replica stream: 256 seeded requests, water boxes of log-uniform 300-30,000 atoms at "
+                          "0.95-1.05 g/cm^3 and 250-400 K (Andersen every 20 steps), 100-5000 steps each (uniform "
+                          "integers), Poisson arrivals at 20 req/s; LJ/DSF at 10 A + the BF16 embedding network at 6 A, "
+                          "dt 0.5 fs; all replica state device-resident, HBM-budget admission"),
 }
 
 
@@ -167,6 +172,69 @@ def cpu_reference(wl, steps: int):
             f"threads on a {ncpu}-CPU host")
 
 
+def serve_bench(args, wl):
+    """The served replica stream: requests are submitted at their Poisson arrival times by a host
+    thread while the server's worker runs the resident replicas; throughput is the stream's work
+    over its makespan (first arrival to last completion, host clock, as a client sees it) and
+    latency is completion time minus arrival time per request."""
+    import torch
+    import cases
+    from nnpengine_b200 import engine as E
+    from nnpengine_b200 import nnp_model as NM
+    from nnpengine_b200 import systems as S
+    from nnpengine_b200.serve import Server
+    nreq = args.serve_requests
+    trace = S.serving_trace(nreq, seed=3)
+    for t in trace:
+        t["nsteps"] = max(20, int(round(t["nsteps"] * args.serve_scale)))
+    boxes = [S.water_request_box(t["natom"], t["density"], t["seed"], t["temperature"]) for t in trace]
+    r, F, U = S.water_lj_table(10.0, 1000)
+    F, U = cases.table_as_loaded(F, U)
+    free, total = torch.cuda.mem_get_info()
+    budget = int(min(0.8 * free, 120e9))
+    srv = Server(0, ntype=2, table=(F, U), bcoef=[E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)],
+                 acoef=[E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)], nnp=NM.embed_model(), bf16=True,
+                 chunk_steps=20, dt=0.5, max_replicas=args.serve_slots, hbm_budget=budget)
+    # warm-up requests (module loading, first graph captures), untimed
+    warm = [srv.submit(S.water_request_box(n, 1.0, 90 + k, 300.0), 40, 300.0, k)
+            for k, n in enumerate([300, 3000, 30000][:max(1, args.warmup)])]
+    for w in warm:
+        srv.wait(w, 600)
+    ids = [None] * nreq
+    t_arr = [0.0] * nreq
+
+    def submitter():
+        t0 = time.perf_counter()
+        for k, (t, b) in enumerate(zip(trace, boxes)):
+            delay = t["t"] - trace[0]["t"] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            t_arr[k] = time.perf_counter()
+            ids[k] = srv.submit(b, t["nsteps"], t["temperature"], t["seed"])
+
+    with ClockSampler(0) as clk:
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        srv.drain(3600)
+    t_end = time.perf_counter()
+    # the server clock (t_submit/t_done) and the host clock differ by a constant offset per request
+    stats = [srv.stats(i) for i in ids]
+    lat = np.array([st["t_done"] - st["t_submit"] for st in stats])
+    ok = sum(1 for st in stats if st["status"] == 2)
+    first_submit = min(st["t_submit"] for st in stats)
+    makespan = max(st["t_done"] for st in stats) - first_submit
+    steps = sum(t["nsteps"] for t in trace)
+    atom_steps = sum(t["nsteps"] * b.natom for t, b in zip(trace, boxes))
+    info = srv.info()
+    srv.close()
+    return dict(replica_steps_per_s=steps / makespan, atom_steps_per_s=atom_steps / makespan, makespan_s=makespan,
+                p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)), mean_s=float(lat.mean()),
+                completed=ok, requests=nreq, total_steps=steps, total_atom_steps=atom_steps,
+                peak_resident=info["peak_resident"], peak_bytes=info["peak_bytes"], hbm_budget=budget,
+                clocks=clk.summary(), wall_after_last_submit_s=t_end - t_arr[-1])
+
+
 def time_enqueue(e, stream, which, reps):
     import torch
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -192,6 +260,9 @@ def main():
     ap.add_argument("--exact", action="store_true", help="pair forces in the reference's exact float sequence")
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--equil", type=int, default=5000)
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="multiply every request's step count")
+    ap.add_argument("--serve-slots", type=int, default=64)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -202,7 +273,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        rate, threads, sample = cpu_reference(wl, args.cpu_steps)
+        cwl = (WORKLOADS["water3k-classical"] | {"nnp": "bf16"}) if wl.get("serve") else wl
+        rate, threads, sample = cpu_reference(cwl, args.cpu_steps)
         print(json.dumps({
             "impl": "reference", "metric": "atom-steps/s", "value": rate, "unit": "atom-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -214,6 +286,30 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if wl.get("serve"):
+        if rank != 0:
+            return
+        res = serve_bench(args, wl)
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                rate, threads, sample = cpu_reference(WORKLOADS["water3k-classical"] | {"nnp": "bf16"}, args.cpu_steps)
+                cpu = {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+                       "sample": sample + "; the reference runs one system per process, so a stream is sequential runs"}
+            except Exception as ex:
+                cpu = {"value": None, "unit": "atom-steps/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {ex}"}
+        print(json.dumps({
+            "metric": "replica-steps/s", "value": res["replica_steps_per_s"], "unit": "replica-steps/s", "n_gpus": 1,
+            "steps": res["total_steps"], "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded request stream)",
+            "config": {"workload": args.workload, "description": wl["desc"], "serve_scale": args.serve_scale,
+                       "slots": args.serve_slots, "timing": "host clock: first arrival to last completion"},
+            "latency_s": {"p50": res["p50_s"], "p99": res["p99_s"], "mean": res["mean_s"]},
+            "serving": res, "cpu_baseline": cpu, "clocks": res["clocks"],
+            "e2e": {"value": res["replica_steps_per_s"], "unit": "replica-steps/s",
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "every request's system goes host->device at admission and its final state device->host"}}))
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist_mod
