@@ -75,10 +75,15 @@ int nnpe_set_system(nnpe_ctx* ctx, int natom, int ntype, double bl, const int* t
 /* Parses the reference's initial-configuration file and its molecule files. */
 int nnpe_load_system_file(nnpe_ctx* ctx, const char* init_file);
 int nnpe_natom(const nnpe_ctx* ctx);
+/* Atom types and molecule ids (atom-id order, int [natom]; NULL to skip) and the box edge. */
+int nnpe_atom_info(const nnpe_ctx* ctx, int* typ, int* mol_id, double* bl);
 int nnpe_npair(const nnpe_ctx* ctx);
 /* Positions/velocities in atom-id order, float [natom*3]; replace the state in place. */
 int nnpe_set_positions(nnpe_ctx* ctx, const float* x);
 int nnpe_set_velocities(nnpe_ctx* ctx, const float* v);
+/* ENVIRON::initV (environ.cpp:190-205): with probability frac per atom, Maxwell-Boltzmann
+ * velocities at `temperature` [K]; the generator is seeded (the reference seeds from random_device). */
+int nnpe_init_velocities(nnpe_ctx* ctx, double temperature, double frac, uint64_t seed);
 
 /* ---- cutoffs, grid and stencils (replaces ENVIRON::init_grid environ.cpp:143-155,
  *      LOCAL::set_ghost_lim environ.h:142, NEIGHLIST::build_bin_list neighlist.cpp:35-168,

@@ -15,6 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib")
 LIB = os.path.join(OUT, "libnnpe.so")
+DRIVER = os.path.join(OUT, "nnpe_run")
+CXX = os.environ.get("CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr",
@@ -51,7 +53,7 @@ def _compile(unit: str, flags, verbose: bool) -> str:
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OUT, exist_ok=True)
     srcs = [os.path.join(CSRC, u) for u in UNITS] + [os.path.join(CSRC, "internal.cuh"), os.path.join(CSRC, "nnp.cuh"), os.path.join(CSRC, "tc_util.cuh"),
-                                                     os.path.join(HERE, "..", "include", "nnpe.h")]
+                                                     os.path.join(HERE, "..", "include", "nnpe.h"), os.path.join(CSRC, "nnpe_run.cpp")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) > max(os.path.getmtime(s) for s in srcs):
         return LIB
     with ThreadPoolExecutor(max_workers=8) as ex:
@@ -60,6 +62,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stderr)
+    # the run-file driver: plain C++ host code over the C ABI, found next to the library at run time
+    cmd = [CXX, "-std=c++17", "-O2", "-Wall", "-o", DRIVER, os.path.join(CSRC, "nnpe_run.cpp"), "-L" + OUT, "-lnnpe",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nnpe_run failed to build:\n" + r.stderr)
     return LIB
 
 

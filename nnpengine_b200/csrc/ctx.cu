@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <random>
 #include <mutex>
 #include <unordered_map>
 #include <string>
@@ -236,6 +237,33 @@ int nnpe_set_positions(nnpe_ctx* c, const float* x) {
   int one = 1;
   NNPE_CUDA(c, cudaMemcpy(c->d_ctrl + CTRL_REBUILD, &one, sizeof(int), cudaMemcpyHostToDevice));
   return NNPE_OK;
+}
+
+int nnpe_atom_info(const nnpe_ctx* c, int* typ, int* mol_id, double* bl) {
+  if (!c || !c->have_system) return NNPE_EARG;
+  if (typ) std::copy(c->h_typ.begin(), c->h_typ.end(), typ);
+  if (mol_id) std::copy(c->h_mol_id.begin(), c->h_mol_id.end(), mol_id);
+  if (bl) *bl = c->bl;
+  return NNPE_OK;
+}
+
+// ENVIRON::initV (environ.cpp:190-205): each atom, with probability `frac`, gets velocity
+// components drawn from N(0, sqrt(T/300 * 300 / m) * kT_m_sqrt); a seeded 64-bit Mersenne twister
+// stands in for the reference's random_device-seeded generator (mathlib.cpp:6-19).
+int nnpe_init_velocities(nnpe_ctx* c, double temperature, double frac, uint64_t seed) {
+  if (!c || !c->have_system || temperature < 0) return nnpe_fail(c, NNPE_EARG, "nnpe_init_velocities");
+  std::vector<float> v((size_t)c->natom * 3, 0.f);
+  if (frac < 1) TRY(nnpe_get_velocities(c, v.data()));
+  std::mt19937_64 gen(seed);
+  std::uniform_real_distribution<double> uni(0.0, 1.0);
+  std::normal_distribution<double> nrm(0.0, 1.0);
+  const double kTmSqrt = 0.0009118367518929329;   // environ.h:80
+  for (int i = 0; i < c->natom; ++i) {
+    if (uni(gen) >= frac) continue;
+    const double fc = std::sqrt(temperature / c->h_mass[i]) * kTmSqrt;
+    for (int d = 0; d < 3; ++d) v[(size_t)i * 3 + d] = (float)(fc * nrm(gen));
+  }
+  return nnpe_set_velocities(c, v.data());
 }
 
 int nnpe_set_velocities(nnpe_ctx* c, const float* v) {

@@ -412,13 +412,14 @@ int forces_enqueue(nnpe_ctx* c, bool ev) {
 }
 
 int energy_reduce_enqueue(nnpe_ctx* c, int mode) {
-  // mode 0: energies only; 1: energies + kinetic into the log; 2: kinetic only (no log)
+  // mode 0: energies only; 1: energies + kinetic into the log; 2: kinetic only (no log);
+  // 3: energies into the log with the kinetic energy of the last thermostat step
   const double* enet = c->nnp ? nnp_atom_energy_ptr(c) : nullptr;
   const int nnet = enet ? c->natom : 0;
   const bool bonded = c->d_mol_terms && (c->nbond + c->nangle + c->ndih) > 0;
   k_reduce<<<1, 1024, 0, c->stream>>>(c->d_eatom, c->d_watom, c->d_kin, c->d_emol, c->d_wmol, enet, c->natom,
-                                      bonded || mode >= 0 ? c->nmol : 0, nnet, mode >= 1, c->d_red, c->d_log,
-                                      c->log_cap, c->d_ctrl, mode == 1);
+                                      bonded || mode >= 0 ? c->nmol : 0, nnet, mode == 1 || mode == 2, c->d_red,
+                                      c->d_log, c->log_cap, c->d_ctrl, mode == 1 || mode == 3);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

@@ -200,10 +200,15 @@ static int enqueue_step(nnpe_ctx* c, int variant) {
     // run.cpp:298: the potential table is refreshed on log steps when gamma != 1
     if (int rc = gr_step_enqueue(c, gr_long, f_log && rmdf_potential_on_log(c))) return rc;
   if (int rc = forces_enqueue(c, f_log)) return rc;
-  if (int rc = verlet_v_enqueue(c, f_log || thermo)) return rc;
-  if (f_log || thermo) {
-    // kinetic energy (and on log steps the potential energy) before the thermostat acts
-    if (int rc = energy_reduce_enqueue(c, f_log ? 1 : 2)) return rc;
+  // The kinetic energy is computed on thermostat steps, before the thermostat acts, and a log step
+  // reports the one of the last thermostat step (run.cpp:349-359, 380); without a thermostat every
+  // log step computes its own.
+  const bool kin_now = thermo || (f_log && c->thermo_kind == 0);
+  if (int rc = verlet_v_enqueue(c, kin_now)) return rc;
+  if (f_log) {
+    if (int rc = energy_reduce_enqueue(c, kin_now ? 1 : 3)) return rc;
+  } else if (thermo) {
+    if (int rc = energy_reduce_enqueue(c, 2)) return rc;
   }
   if (thermo)
     if (int rc = thermostat_enqueue(c)) return rc;

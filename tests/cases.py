@@ -100,3 +100,45 @@ def write_nnp_inputs(m, d):
     b, a, dd = water_bonded_raw()
     NM.write_weight_file(wt, m, b, a, dd)
     return dict(model=model, param=param, wt=wt)
+
+
+def write_run_input(d, mode, s, table=None, nnp_paths=None, temps=(0.0, 0.0), steps=(20, 5, 20, 5, 10),
+                    rmdf=None, nbin=1000, cutoffs=(10.0, 2.0, 10.0), nq=512, qmax=20.0):
+    """The run input file of the reference's `classical` or `nnp_run` mode (run.cpp:25-50) for a
+    case in directory d; rmdf = (strength, gamma, target file) or None (no target: n_sq 0, which
+    the reference reads but cannot run, so its harness runs use one target of strength 0)."""
+    os.makedirs(d, exist_ok=True)
+    init = os.path.join(d, "init.txt")
+    S.write_init_file(init, s)
+    lines = [init, "%g %g %g" % cutoffs]
+    if mode == "classical":
+        tab = os.path.join(d, "table.txt")
+        S.write_pair_table(tab, table[0], table[1], table[2])
+        lines += [f"{nbin} {tab}", "1", f"1.0 {WATER_BOND_K}", "1", f"109.47 0 0 {WATER_ANGLE_KC}", "0"]
+    else:
+        lines += ["1", "1", "0", nnp_paths["param"], nnp_paths["wt"], str(nbin)]
+    lines.append(f"{nbin} {nq} {qmax}")
+    if rmdf is None:
+        lines += ["0 1", "0", "*"]
+    else:
+        lines += [f"{rmdf[0]} {rmdf[1]}", f"1 {rmdf[2]}", os.path.join(d, "no_such_delta.txt")]
+    lines.append(f"{temps[0]} {temps[1]}")
+    lines.append(" ".join(str(v) for v in steps))
+    out = {k: os.path.join(d, k + ".out") for k in ("xyz", "gr", "sq", "sqx", "force")}
+    lines += [f"{out['xyz']} 0", f"{out['gr']} 0", f"{out['sq']} 0", "* 0 20 10", f"{out['sqx']} 0"]
+    if mode == "classical":
+        lines.append(f"{out['force']} 0")
+    path = os.path.join(d, "run.in")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path, out
+
+
+def parse_log(text):
+    """The step lines of the reference's log (run.cpp:383-390): md_step temp press erg dif nbuild."""
+    rows = []
+    for line in text.splitlines():
+        f = line.split()
+        if len(f) == 6 and f[0].lstrip("-").isdigit():
+            rows.append([float(v) for v in f])
+    return np.array(rows)

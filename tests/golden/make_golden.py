@@ -20,6 +20,12 @@ is run on the seeded cases of tests/cases.py; its outputs are stored compactly:
                  g(r) steps every 5 steps (cell-based every 10): per-log-step penalty, final x, v
                  and tables.
 
+* driver648.npz  the reference's own executable (oracle/_ref/nnp.exe: run.cpp + main.cpp, unmodified)
+                 on run input files of both modes for the 648-atom water box at 0 K (so that the
+                 first log line does not depend on its unseeded generator): the classical mode with
+                 RMDF (strength 0.02, gamma 0.5) and the nnp_run mode with the tabulated NNP and RMDF
+                 on its pair tables; its log lines and the line counts of its output files.
+
 Run:  python tests/golden/make_golden.py   (needs /root/reference/src and `make -C oracle ref`).
 """
 from __future__ import annotations
@@ -109,6 +115,30 @@ def rmdf2000(work):
     print("rmdf2000: penalty", float(snap["rmdf_erg"][0]), "md penalties", md["log_exp"])
 
 
+def driver648(work):
+    import subprocess
+    from nnpengine_b200 import nnp_model as NM
+    out = {}
+    for mode in ("classical", "nnp_run"):
+        d = os.path.join(work, mode)
+        os.makedirs(d, exist_ok=True)
+        s, table = cases.water_case()
+        tpath, _ = rmdf_target(d)
+        if mode == "classical":
+            path, files = cases.write_run_input(d, mode, s, table, rmdf=(RMDF_STRENGTH, RMDF_GAMMA, tpath))
+        else:
+            paths = cases.write_nnp_inputs(NM.gauss_model(), d)
+            path, files = cases.write_run_input(d, mode, s, nnp_paths=paths, rmdf=(RMDF_STRENGTH, RMDF_GAMMA, tpath),
+                                                nbin=750, cutoffs=(6.0, 2.0, 6.0))
+        r = subprocess.run([os.path.join(orc.REF_DIR, "nnp.exe"), mode, path], capture_output=True, text=True,
+                           timeout=600, check=True)
+        out[f"{mode}_log"] = cases.parse_log(r.stdout)
+        out[f"{mode}_lines"] = np.array([sum(1 for _ in open(files[k])) if os.path.exists(files[k]) else 0
+                                         for k in ("xyz", "gr", "sq", "sqx", "force")])
+        print(f"driver648 {mode}: step 0 {out[f'{mode}_log'][0]}, output lines {out[f'{mode}_lines']}")
+    np.savez_compressed(os.path.join(HERE, "driver648.npz"), **out)
+
+
 def nnp_gauss648(work):
     from nnpengine_b200 import nnp_model as NM
     s, table = cases.water_case()
@@ -133,3 +163,4 @@ if __name__ == "__main__":
         mixture2000(os.path.join(t, "m"))
         nnp_gauss648(os.path.join(t, "n"))
         rmdf2000(os.path.join(t, "r"))
+        driver648(os.path.join(t, "d"))

@@ -1,0 +1,61 @@
+"""The C++ run-file driver (nnpe_run, the reference's `classical` and `nnp_run` step loops on the
+device) against the reference's own executable on the same input files.
+
+Both runs start at 0 K, so their first log line (forces and energies of the starting
+configuration, the kinetic energy after the first updateV, the RMDF penalty of the first g(r)
+step) does not depend on the reference's unseeded random generator; later lines do (its Andersen
+thermostat picks atoms at random), so for those the driver's log is checked for its form and the
+output files for the reference's layout.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases
+from nnpengine_b200 import build
+from nnpengine_b200 import nnp_model as NM
+from nnpengine_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+STRENGTH, GAMMA = 0.02, 0.5
+
+
+def run_case(tmp_path, mode):
+    d = str(tmp_path / mode)
+    os.makedirs(d, exist_ok=True)
+    s, table = cases.water_case()
+    q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, 2, seed=7)
+    tpath = os.path.join(d, "sq_target.txt")
+    S.write_sq_target(tpath, q, sqex, wt, ff)
+    if mode == "classical":
+        path, files = cases.write_run_input(d, mode, s, table, rmdf=(STRENGTH, GAMMA, tpath))
+    else:
+        paths = cases.write_nnp_inputs(NM.gauss_model(), d)
+        path, files = cases.write_run_input(d, mode, s, nnp_paths=paths, rmdf=(STRENGTH, GAMMA, tpath), nbin=750,
+                                            cutoffs=(6.0, 2.0, 6.0))
+    r = subprocess.run([build.DRIVER, mode, path, "--seed", "5", "--fp32-state"], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return cases.parse_log(r.stdout), files
+
+
+@pytest.mark.parametrize("mode", ["classical", "nnp_run"])
+def test_driver_first_log_line_matches_reference(tmp_path, mode):
+    g = np.load(os.path.join(cases.GOLDEN, "driver648.npz"))
+    log, files = run_case(tmp_path, mode)
+    ref = g[f"{mode}_log"]
+    assert log.shape == ref.shape                       # the same log steps
+    np.testing.assert_array_equal(log[:, 0], ref[:, 0])
+    step0, ref0 = log[0], ref[0]
+    np.testing.assert_allclose(step0[1], ref0[1], rtol=1e-4)     # temperature after the first updateV
+    np.testing.assert_allclose(step0[2], ref0[2], rtol=1e-4)     # pressure
+    np.testing.assert_allclose(step0[3], ref0[3], rtol=1e-5)     # potential energy
+    np.testing.assert_allclose(step0[4], ref0[4], rtol=1e-3)     # RMDF penalty (float vs FP64 S(q))
+    assert step0[5] == ref0[5]                                   # list builds
+    assert np.all(np.isfinite(log))
+    lines = [sum(1 for _ in open(files[k])) if os.path.exists(files[k]) else 0
+             for k in ("xyz", "gr", "sq", "sqx", "force")]
+    np.testing.assert_array_equal(lines, g[f"{mode}_lines"])
