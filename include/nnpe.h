@@ -132,6 +132,13 @@ int nnpe_set_total_steps(nnpe_ctx* ctx, int total_steps);
 int nnpe_thermostat(nnpe_ctx* ctx, int kind, double t_start, double t_end, int interval, double frac,
                     uint64_t seed);
 
+/* Single operations of the step for a caller that keeps the reference's own loop (nnpe.hpp):
+ * VERLET::updateX with the given dt (the first call also clears the accelerations, run.cpp:220-221;
+ * an atom that moved more than skin/2 since the last build marks the list invalid), and
+ * VERLET::updateV with the kinetic energy (VERLET::computeKE, FP64 sum) when ekin != NULL. */
+int nnpe_verlet_update_x(nnpe_ctx* ctx, double dt);
+int nnpe_verlet_update_v(nnpe_ctx* ctx, double* ekin);
+
 /* ---- the neighbour list (NEIGHLIST, neighlist.h:6-47) ---------------------------------- */
 /* Rebuild: refold_and_tag, sort, generate_ghost, tidyup_ghost, update_ghost_pos<true>,
  * sort_ghost, update_ghost_and_info, build (run.cpp:249-276). */
@@ -248,9 +255,10 @@ int nnpe_rmdf_set(nnpe_ctx* ctx, int n_sq, const double* sqex, const double* wt,
 int nnpe_rmdf_load(nnpe_ctx* ctx, int n_sq, const char* const* files, double strength, double gamma);
 /* RMDF::loadDeltaSQ (grsq.cpp:1419-1443); a missing file is ignored, as there. */
 int nnpe_rmdf_load_delta(nnpe_ctx* ctx, const char* fname);
-/* One update on the current S(q): compute_Qspace, compute_Rspace, compute_Potential if potential;
- * erg_exp = the penalty times natom/4 (grsq.cpp:1117). */
-int nnpe_rmdf_step(nnpe_ctx* ctx, int potential, double* erg_exp);
+/* Parts of one update on the current S(q), as bits of `parts`: 1 compute_Qspace (erg_exp = the
+ * penalty times natom/4, grsq.cpp:1117), 2 compute_Rspace, 4 compute_Potential (the _NNP variants
+ * when the network's tables are refined). */
+int nnpe_rmdf_step(nnpe_ctx* ctx, int parts, double* erg_exp);
 /* Weighted S_n(q), deltaS_n(q) [n_sq][nq] and force_q [npair][nq] of the last update (NULL to skip). */
 int nnpe_rmdf_get(nnpe_ctx* ctx, double* sq, double* deltasq, double* force_q);
 /* RMDF::dumpSQ (grsq.cpp:1380-1416). */

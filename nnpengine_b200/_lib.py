@@ -68,6 +68,9 @@ _SIGS = {
     "nnpe_get_velocities": (C.c_int, [_vp, _f32p]),
     "nnpe_get_velocities_f64": (C.c_int, [_vp, _f64p]),
     "nnpe_get_atom_energy": (C.c_int, [_vp, _f64p]),
+    "nnpe_verlet_update_x": (C.c_int, [_vp, C.c_double]),
+    "nnpe_verlet_update_v": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "nnpe_init_velocities": (C.c_int, [_vp, C.c_double, C.c_double, C.c_uint64]),
     "nnpe_run": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(Thermo), C.c_int, C.POINTER(C.c_int)]),
     "nnpe_run_graph": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(Thermo), C.c_int, C.POINTER(C.c_int)]),
     "nnpe_nnp_set": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,

@@ -257,6 +257,39 @@ static int prepare_run(nnpe_ctx* c, int max_log) {
   return 0;
 }
 
+// VERLET::updateX (verlet.cpp:29-43) with an explicit dt; the first call also performs what
+// run.cpp:220-221 does before its first updateX (clear f) and takes the loaded state as FP32
+// coordinates. Marks the list for a rebuild when an atom moved more than skin/2 since the last
+// build (the check NEIGHLIST::isvalid reads).
+extern "C" int nnpe_verlet_update_x(nnpe_ctx* c, double dt) {
+  if (!c || !c->have_setup || !c->d_pos) return nnpe_fail(c, NNPE_EARG, "nnpe_verlet_update_x: not set up");
+  cudaSetDevice(c->device);
+  if (!c->first_step_done) {
+    NNPE_CUDA(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float4) * c->natom, c->stream));
+    k_init_pos<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_xd, c->d_qm, c->d_pos, c->natom);
+    int one = 1;
+    NNPE_CUDA(c, cudaMemcpyAsync(c->d_ctrl + CTRL_REBUILD, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    c->first_step_done = true;
+  }
+  if (int rc = verlet_x_enqueue(c, dt, true)) return rc;
+  return nnpe_sync_errors(c);
+}
+
+// VERLET::updateV (verlet.cpp:46-61) on the forces of the last evaluation, and the kinetic energy
+// (VERLET::computeKE, verlet.cpp:87-97, summed over all atoms in FP64) when ekin != NULL.
+extern "C" int nnpe_verlet_update_v(nnpe_ctx* c, double* ekin) {
+  if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_verlet_update_v: not set up");
+  cudaSetDevice(c->device);
+  if (int rc = verlet_v_enqueue(c, ekin != nullptr)) return rc;
+  if (ekin) {
+    if (int rc = energy_reduce_enqueue(c, 2)) return rc;
+    NNPE_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (int rc = nnpe_sync_errors(c)) return rc;
+  if (ekin) *ekin = c->h_red[2];
+  return NNPE_OK;
+}
+
 static int finish_run(nnpe_ctx* c, nnpe_thermo* log, int max_log, int* nlog) {
   if (int rc = nnpe_sync_errors(c)) return rc;
   const int n = std::min(c->h_ctrl[CTRL_NLOG], max_log);

@@ -134,16 +134,18 @@ void rmdf_free(nnpe_ctx* c) {
   c->rmdf = nullptr;
 }
 
-// compute_Qspace + compute_Rspace (+ compute_Potential when `potential`) on the S(q) of the last
-// g(r) step; erg_exp lands in d_red[4].
-int rmdf_step_enqueue(nnpe_ctx* c, bool potential) {
+// Parts of an update on the S(q) of the last g(r) step (bit 1 compute_Qspace, 2 compute_Rspace,
+// 4 compute_Potential); erg_exp lands in d_red[4].
+static int rmdf_parts_enqueue(nnpe_ctx* c, int parts) {
   RmdfState* r = c->rmdf;
   if (!r) return 0;
-  k_rmdf_q<<<1, 512, 0, c->stream>>>(c->d_sq, r->d_sqwt, r->d_fwt, r->d_sqex, r->d_wt, r->d_dsq, r->d_sqn, r->d_fq, r->n_sq,
-                                     r->P, r->nq, r->gamma, (double)c->natom, c->d_red);
+  if (parts & 1)
+    k_rmdf_q<<<1, 512, 0, c->stream>>>(c->d_sq, r->d_sqwt, r->d_fwt, r->d_sqex, r->d_wt, r->d_dsq, r->d_sqn, r->d_fq,
+                                       r->n_sq, r->P, r->nq, r->gamma, (double)c->natom, c->d_red);
   float2* tbl = rmdf_table(c);
   const int warps = r->P * r->nbin, blocks = nblocks((long)warps * 32, 256);
-  for (int comp = 0; comp < (potential ? 2 : 1); ++comp) {
+  for (int comp = 0; comp < 2; ++comp) {
+    if (!(parts & (comp == 0 ? 2 : 4))) continue;
     const double* mx = comp == 0 ? r->d_ftmx : r->d_potmx;
     if (r->nnp) k_rmdf_r<true><<<blocks, 256, 0, c->stream>>>(r->d_fq, mx, r->d_base, tbl, r->P, r->nbin, r->nq, comp);
     else k_rmdf_r<false><<<blocks, 256, 0, c->stream>>>(r->d_fq, mx, r->d_base, tbl, r->P, r->nbin, r->nq, comp);
@@ -151,6 +153,9 @@ int rmdf_step_enqueue(nnpe_ctx* c, bool potential) {
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }
+
+// compute_Qspace + compute_Rspace (+ compute_Potential) of a g(r) step of the loop.
+int rmdf_step_enqueue(nnpe_ctx* c, bool potential) { return rmdf_parts_enqueue(c, potential ? 7 : 3); }
 
 bool rmdf_potential_on_log(const nnpe_ctx* c) { return c->rmdf && c->rmdf->gamma != 1.0; }
 
@@ -261,12 +266,12 @@ extern "C" int nnpe_rmdf_load(nnpe_ctx* c, int n_sq, const char* const* files, d
   return nnpe_rmdf_set(c, n_sq, sqex.data(), wt.data(), ff.data(), strength, gamma);
 }
 
-// One refinement update on the current g(r) (tally + S(q) of the last call to nnpe_sq_compute or of
-// the step loop): compute_Qspace, compute_Rspace, and compute_Potential when potential != 0.
-extern "C" int nnpe_rmdf_step(nnpe_ctx* c, int potential, double* erg_exp) {
+// Parts of one refinement update on the current g(r) (tally + S(q) of the last call to
+// nnpe_sq_compute or of the step loop).
+extern "C" int nnpe_rmdf_step(nnpe_ctx* c, int parts, double* erg_exp) {
   if (!c || !c->rmdf) return nnpe_fail(c, NNPE_EARG, "nnpe_rmdf_step: no RMDF set up");
   cudaSetDevice(c->device);
-  if (int rc = rmdf_step_enqueue(c, potential != 0)) return rc;
+  if (int rc = rmdf_parts_enqueue(c, parts)) return rc;
   if (erg_exp) NNPE_CUDA(c, cudaMemcpyAsync(erg_exp, c->d_red + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
   return NNPE_OK;

@@ -281,8 +281,9 @@ class Engine:
         self._ok(self.lib.nnpe_rmdf_load(self.h, len(files), arr, strength, gamma))
 
     def rmdf_step(self, potential: bool = False) -> float:
+        """compute_Qspace + compute_Rspace (+ compute_Potential); returns erg_exp."""
         e = C.c_double(0)
-        self._ok(self.lib.nnpe_rmdf_step(self.h, int(potential), C.byref(e)))
+        self._ok(self.lib.nnpe_rmdf_step(self.h, 7 if potential else 3, C.byref(e)))
         return e.value
 
     def rmdf_get(self):

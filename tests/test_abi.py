@@ -1,5 +1,6 @@
 """The C-ABI library: it loads, exports every declared symbol, and fails cleanly without a GPU."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -75,3 +76,29 @@ def test_serving_struct_layout_matches_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def _build_adapter_loop(out_dir):
+    import os
+    import subprocess
+    from nnpengine_b200 import build
+    here = os.path.dirname(os.path.abspath(__file__))
+    inc = os.path.join(here, "..", "include")
+    exe = os.path.join(out_dir, "adapter_loop")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", inc, os.path.join(here, "adapter_loop.cpp"),
+                    "-L", build.OUT, "-lnnpe", "-Wl,-rpath," + build.OUT, "-o", exe], check=True)
+    return exe
+
+
+def test_reference_classes_adapter_compiles(tmp_path):
+    """A loop written like run.cpp against the reference's class names compiles and links against
+    include/nnpe.hpp and libnnpe.so (it runs in the GPU tests)."""
+    import shutil
+    if not shutil.which("g++"):
+        pytest.skip("no C++ compiler")
+    assert os.path.exists(_build_adapter_loop(str(tmp_path)))
+
+
+def test_run_file_driver_built():
+    from nnpengine_b200 import build
+    assert os.path.exists(build.DRIVER) and os.access(build.DRIVER, os.X_OK)

@@ -52,10 +52,40 @@ def test_driver_first_log_line_matches_reference(tmp_path, mode):
     step0, ref0 = log[0], ref[0]
     np.testing.assert_allclose(step0[1], ref0[1], rtol=1e-4)     # temperature after the first updateV
     np.testing.assert_allclose(step0[2], ref0[2], rtol=1e-4)     # pressure
-    np.testing.assert_allclose(step0[3], ref0[3], rtol=1e-5)     # potential energy
+    # potential energy: the reference sums it in float per thread; on this box its total of ~15
+    # kcal/mol is the small difference of terms of ~1e4, and the float sums carry ~1e-3 of that
+    np.testing.assert_allclose(step0[3], ref0[3], rtol=1e-5, atol=0.02)
     np.testing.assert_allclose(step0[4], ref0[4], rtol=1e-3)     # RMDF penalty (float vs FP64 S(q))
     assert step0[5] == ref0[5]                                   # list builds
     assert np.all(np.isfinite(log))
     lines = [sum(1 for _ in open(files[k])) if os.path.exists(files[k]) else 0
              for k in ("xyz", "gr", "sq", "sqx", "force")]
     np.testing.assert_array_equal(lines, g[f"{mode}_lines"])
+
+
+def test_reference_style_loop_through_adapter_matches_step_loop(tmp_path):
+    """run.cpp's classical loop written against nnpe.hpp (one device call per reference call) gives
+    the same bits as the library's own step loop on the same system."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_abi import _build_adapter_loop
+    from nnpengine_b200 import engine as E
+    exe = _build_adapter_loop(str(tmp_path))
+    s, table = cases.water_case()
+    f = cases.write_inputs(s, table, str(tmp_path / "in"))
+    xout = str(tmp_path / "x.f32")
+    r = subprocess.run([exe, f["init"], f["table"], "20", "5", xout], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    log = cases.parse_log(r.stdout)
+    x_adapter = np.fromfile(xout, np.float32).reshape(-1, 3)
+    e = E.Engine(0)
+    e.load_system_file(f["init"])
+    e.setup(10.0, 2.0, 10.0, 2048)
+    e._ok(e.lib.nnpe_pair_load_table(e.h, 1000, f["table"].encode()))
+    e._ok(e.lib.nnpe_bonded_autogen(e.h, 1, E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K), 1,
+                                    E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC), 0, np.zeros(4, np.float32)))
+    e.verlet(1.0, True)
+    ref = e.run(21, log_interval=5)
+    np.testing.assert_array_equal(x_adapter, e.positions())
+    np.testing.assert_allclose(log[:, 3], [r["erg"] for r in ref], rtol=1e-6)
+    e.close()
