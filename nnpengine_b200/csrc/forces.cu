@@ -28,11 +28,19 @@ struct PairParams {
   int N, cap, ntype, nbin;
   float cutoff, cutsq, r_dr, vc, fc;
   bool accumulate;
+  // the network term's pair list, filtered here from the same distances (nullptr: not wanted)
+  uint32_t* list6;
+  int* n6;
+  int cap6;
+  float cut6sq;
+  int* ctrl;
 };
 
 // One warp per atom: lanes stride over the atom's list row (coalesced 128-byte reads), gather
 // neighbour positions, and reduce with shuffles; the warp writes the atom's force once (no
-// atomics, deterministic).
+// atomics, deterministic). With list6 set, the entries inside the network cutoff (the same float
+// rsq, the reference's `rsq < cutsq` of pair_nnp.cpp:656) are compacted in list order into the
+// network's pair list on the way, so the list is read once per step.
 // Exact double coordinates of list entry j: a real atom's float position, or its owner's float
 // position plus the float box shift added in double (the image the float list entry rounds).
 __device__ __forceinline__ double3 exact_pos(const PairParams& p, int j) {
@@ -82,12 +90,34 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
   const int n = p.ncount[i];
   float fx = 0.f, fy = 0.f, fz = 0.f;
   double e = 0.0, w = 0.0;
-  for (int k = lane; k < n; k += 32) {
-    const uint32_t ent = __ldg(row + k);
+  uint32_t* out6 = p.list6 ? p.list6 + (size_t)i * p.cap6 : nullptr;
+  int cnt6 = 0;
+  // software pipeline over 32-entry chunks: the list entries two chunks ahead and the neighbour
+  // positions one chunk ahead are in flight while a chunk is evaluated
+  uint32_t e_nx = lane < n ? __ldg(row + lane) : 0u;
+  uint32_t e_nx2 = lane + 32 < n ? __ldg(row + lane + 32) : 0u;
+  float4 x_nx = lane < n ? __ldg(p.pos + (e_nx & NNPE_J_MASK)) : xi;
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    const bool in = k < n;
+    const uint32_t ent = e_nx;
+    const float4 xj = x_nx;
+    e_nx = e_nx2;
+    x_nx = k + 32 < n ? __ldg(p.pos + (e_nx & NNPE_J_MASK)) : xi;
+    e_nx2 = k + 64 < n ? __ldg(row + k + 64) : 0u;
     const int j = (int)(ent & NNPE_J_MASK);
-    const float4 xj = __ldg(p.pos + j);
     float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
     const float rsq = dx * dx + dy * dy + dz * dz;
+    if (out6) {   // warp-uniform
+      const bool ok6 = in && rsq < p.cut6sq;
+      const unsigned b6 = __ballot_sync(0xffffffffu, ok6);
+      if (ok6) {
+        const int idx = cnt6 + __popc(b6 & ((1u << lane) - 1));
+        if (idx < p.cap6) out6[idx] = ent;
+      }
+      cnt6 += __popc(b6);
+    }
+    if (!in) continue;
     if (rsq < p.cutsq) {
       const int tj = (ent >> 27) & 7, s = ent >> 30;
       const float2* tab = p.table + (size_t)ptrow[tj] * (p.nbin + 1);
@@ -133,6 +163,10 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
       e += __shfl_xor_sync(0xffffffffu, e, o);
       w += __shfl_xor_sync(0xffffffffu, w, o);
     }
+  }
+  if (out6 && lane == 0) {
+    p.n6[i] = min(cnt6, p.cap6);
+    if (cnt6 > p.cap6) atomicOr(p.ctrl + CTRL_ERR, NNPE_DEV_LIST_OVERFLOW);
   }
   if (lane == 0) {
     if (p.accumulate) {
@@ -356,8 +390,11 @@ __global__ void __launch_bounds__(1024) k_reduce(const double* eatom, const doub
 
 const double* nnp_atom_energy_ptr(nnpe_ctx* c);   // nnp.cu
 bool nnp_enabled(nnpe_ctx* c);
+float nnp_cutoff(nnpe_ctx* c);
 
-int pair_enqueue(nnpe_ctx* c, bool ev) {
+bool nnp_list6(nnpe_ctx* c, uint32_t** list6, int** n6, int* cap6, float* cut6);   // nnp.cu
+
+int pair_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   const int N = c->natom;
   PairParams p;
   p.pos = c->d_pos; p.list = c->d_list; p.ncount = c->d_ncount; p.info = c->d_info; p.table = c->d_table;
@@ -368,6 +405,12 @@ int pair_enqueue(nnpe_ctx* c, bool ev) {
   p.r_dr = (float)c->nbin / c->pair_cutoff;   // LJTableCoulDSF ctor (pair.cpp:176-177)
   p.vc = -1 / p.cutoff; p.fc = p.vc / p.cutoff;  // pair.cpp:191-193 (erfc disabled)
   p.accumulate = false;
+  p.list6 = nullptr; p.n6 = nullptr; p.cap6 = 0; p.cut6sq = 0.f; p.ctrl = c->d_ctrl;
+  if (filter6) {
+    float cut6 = 0.f;
+    nnp_list6(c, &p.list6, &p.n6, &p.cap6, &cut6);
+    p.cut6sq = cut6 * cut6;
+  }
   const int blocks = nblocks((long)N * 32, 128);
   if (c->exact_forces) {
     if (ev) k_pair<true, true><<<blocks, 128, 0, c->stream>>>(p);
@@ -398,14 +441,22 @@ int bonded_enqueue(nnpe_ctx* c, bool ev) {
 }
 
 // The force block: pair (writes the forces), network term (adds), bonded terms (add).
+// The pair kernel filters the network's pairs when both terms run and the network cutoff lies
+// inside the list.
+bool pair_filters_list6(nnpe_ctx* c) {
+  return c->nnp && nnp_enabled(c) && c->pair_on && c->d_table && nnp_cutoff(c) <= c->pair_cutoff + c->skin;
+}
+
 int forces_enqueue(nnpe_ctx* c, bool ev) {
+  const bool net = c->nnp && nnp_enabled(c);
+  const bool fused = pair_filters_list6(c);
   if (c->pair_on && c->d_table) {
-    if (int rc = pair_enqueue(c, ev)) return rc;
+    if (int rc = pair_enqueue(c, ev, fused)) return rc;
   } else {
     k_zero_forces<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_frc, c->d_eatom, c->d_watom, c->natom);
   }
-  if (c->nnp && nnp_enabled(c))
-    if (int rc = nnp_forces_enqueue(c, ev)) return rc;
+  if (net)
+    if (int rc = nnp_forces_enqueue(c, ev, !fused)) return rc;
   if (int rc = bonded_enqueue(c, ev)) return rc;
   NNPE_CHECK_LAUNCH(c);
   return 0;

@@ -381,7 +381,8 @@ extern "C" int nnpe_set_total_steps(nnpe_ctx* c, int total) {
   return NNPE_OK;
 }
 
-int pair_enqueue(nnpe_ctx* c, bool ev);
+int pair_enqueue(nnpe_ctx* c, bool ev, bool filter6);
+bool pair_filters_list6(nnpe_ctx* c);
 int bonded_enqueue(nnpe_ctx* c, bool ev);
 
 // Enqueue one kernel class on the context's stream without synchronising, for timing it with
@@ -390,7 +391,7 @@ int bonded_enqueue(nnpe_ctx* c, bool ev);
 extern "C" int nnpe_profile_enqueue(nnpe_ctx* c, int which) {
   if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_profile_enqueue: not set up");
   switch (which) {
-    case 0: return pair_enqueue(c, false);
+    case 0: return pair_enqueue(c, false, pair_filters_list6(c));
     case 1: {
       int one = 1;
       NNPE_CUDA(c, cudaMemcpyAsync(c->d_ctrl + CTRL_REBUILD, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -398,7 +399,7 @@ extern "C" int nnpe_profile_enqueue(nnpe_ctx* c, int which) {
       return ghost_update_enqueue(c, true);
     }
     case 2: return bonded_enqueue(c, false);
-    case 3: return c->nnp ? nnp_forces_enqueue(c, false) : 0;
+    case 3: return c->nnp ? nnp_forces_enqueue(c, false, !pair_filters_list6(c)) : 0;
     case 4: {
       if (int rc = verlet_x_enqueue(c, 0.0, false)) return rc;
       return verlet_v_enqueue(c, false);

@@ -216,7 +216,7 @@ int thermostat_enqueue(nnpe_ctx* c);
 int gr_tally_enqueue(nnpe_ctx* c, int inner);
 int alloc_state(nnpe_ctx* c);
 int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
-int nnp_forces_enqueue(nnpe_ctx* c, bool ev);
+int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6 = true);
 int nnpe_bonded_coefs(nnpe_ctx* c, const float* bcoef, const float* acoef, const float* dcoef);
 void nnp_free(nnpe_ctx* c);
 // Device allocations of a context go through these two, which keep the context's byte count

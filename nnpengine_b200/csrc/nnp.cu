@@ -54,6 +54,12 @@ void nnp_free(nnpe_ctx* c) {
 
 const double* nnp_atom_energy_ptr(nnpe_ctx* c) { return c->nnp && c->nnp->enabled ? c->nnp->d_enet : nullptr; }
 bool nnp_enabled(nnpe_ctx* c) { return c->nnp && c->nnp->enabled; }
+float nnp_cutoff(nnpe_ctx* c) { return c->nnp ? c->nnp->rc : 0.f; }
+bool nnp_list6(nnpe_ctx* c, uint32_t** list6, int** n6, int* cap6, float* cut6) {
+  if (!c->nnp) return false;
+  *list6 = c->nnp->d_list6; *n6 = c->nnp->d_n6; *cap6 = c->nnp->cap6; *cut6 = c->nnp->rc;
+  return true;
+}
 
 int nnpe_nnp_enable(nnpe_ctx* c, int on) {
   if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_enable: no network");
@@ -644,13 +650,14 @@ int nnp_species_enqueue(nnpe_ctx* c) {
   return 0;
 }
 
-int nnp_forces_enqueue(nnpe_ctx* c, bool ev) {
+int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   NnpModel* m = c->nnp;
   const int N = c->natom;
   cudaStream_t st = c->stream;
   const float cs = m->rc * m->rc;
-  k_filter6<<<nblocks((long)N * 32, 128), 128, 0, st>>>(c->d_pos, c->d_list, c->d_ncount, c->cap, m->d_list6, m->d_n6,
-                                                      m->cap6, cs, N, c->d_ctrl);
+  if (filter6)   // else the pair kernel of this step has filled the list (forces.cu)
+    k_filter6<<<nblocks((long)N * 32, 128), 128, 0, st>>>(c->d_pos, c->d_list, c->d_ncount, c->cap, m->d_list6, m->d_n6,
+                                                        m->cap6, cs, N, c->d_ctrl);
   if (int rc = nnp_species_enqueue(c)) return rc;
   NnpArgs a = make_args(c);
   if (m->bf16) return nnp_tc_forces_enqueue(c, ev);

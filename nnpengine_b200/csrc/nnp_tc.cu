@@ -38,7 +38,8 @@ struct NnpTc {
   int* d_tile_row = nullptr;
   int ntiles = 0;
   int* d_soff = nullptr;
-  int ctas_desc = 1, ctas_force = 1;   // resident CTAs per SM (shared memory, registers, tensor memory)
+  int ctas_desc = 3, ctas_force = 2;   // CTAs per SM in the grid (shared and tensor memory bound)
+  unsigned char* d_wdesc64 = nullptr;  // B image N=64 x K=64: W2_t[q][c] at k=t*32+q (b2 added in the epilogue)
 };
 
 namespace {
@@ -49,6 +50,24 @@ constexpr size_t kImgL1 = 128 * 256 * 2, kImgL2 = 128 * 128 * 2, kImgB2 = 128 * 
 __device__ __forceinline__ float tanh_fast(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Two FP32 values rounded to BF16 and packed (lo in the low half, as __floats2bfloat162_rn does).
+__device__ __forceinline__ uint32_t pack_bf2(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+// tanh of two packed BF16 values (one transcendental-unit operation for both).
+__device__ __forceinline__ uint32_t tanh_bf2(uint32_t x) {
+  uint32_t y;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
+  return y;
+}
+__device__ __forceinline__ uint32_t mul_bf2(uint32_t a, uint32_t b) {
+  uint32_t y;
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(y) : "r"(a), "r"(b));
   return y;
 }
 
@@ -338,6 +357,323 @@ __global__ void __launch_bounds__(128, 8) k_tc_desc(TcArgs a) {
 }
 
 // -------------------------------------------------------------------------------------------
+// Descriptor, pipelined over packed tiles.
+//
+// A CTA owns a contiguous range of atoms. Its pairs (per-atom counts n6) are cut into tiles of at most 128 rows holding at most two atom segments:
+// the rest of atom a (la = 0) and, when that ends inside the tile, the start of atom a+1 (la = 1),
+// so the 8-row one-hot reduction of the descriptor (rows 4 la + s) covers every tile. A
+// segment that runs past the tile end is carried in shared memory to the next tile, and an atom's
+// G is stored once, when its last segment is reduced, so no two CTAs or tiles write it.
+//
+// Per tile t the CTA's 128 threads (row p = thread p) run, in order:
+//   (1) first layer of tile t+1 into operand buffer A[(t+1) % 3]; loads of tile t+2 issued,
+//   (2) barrier, after which MMA 1 of tile t and MMA 2 of tile t-1 are complete,
+//   (3) warp 0: G of tile t-1 out of TMEM[(t-1) % 2], then MMA 1 of tile t+1 into that buffer
+//       (Z = H W2s, K = 64 block-diagonal over the neighbour species; b2 is added in the epilogue),
+//   (4) epilogue of tile t: y = scale cff tanh(z + b2) -> Y (BF16, MN-major) over A[t % 3], and the
+//       one-hot S of the (la, s) rows,
+//   (5) barrier; MMA 2 of tile t: TMEM[t % 2] = S Y.
+// MMA 1 of tile t+1 and MMA 2 of tile t run while the threads compute, so the wait of (2) finds
+// them done; three operand buffers and two TMEM buffers keep every buffer out of reach of the MMA
+// that reads it. The activations are BF16 operands of the next MMA, so their tanh is evaluated on
+// BF16 pairs (one transcendental-unit operation per two values).
+constexpr int kK64 = 64;
+constexpr int kEmbStride4 = 132;   // 16-byte aligned rows of the per-species constants
+constexpr int kDescStages = 3;
+constexpr int kSmemDesc2 = 64 * kK64 * 2 + kDescStages * kTile * kK64 * 2 + 8 * kTile * 2 + 2 * kEmbStride4 * 4 + 256 * 4;
+
+struct DescArgs {
+  const float4* pos;
+  const uint32_t* list6;
+  const int* n6;
+  const int* gowner;
+  const unsigned char* wdesc;   // B of MMA 1: N = 64 channels x K = 64, [W2_0; W2_1]
+  const float* emb_small;       // per species W1[32] b1[32] b2[64] (stride 128)
+  float* G;
+  int* ctrl;
+  int cap6, N, ntype, npos;
+  float rc, scale;
+};
+
+struct TileSeg { int a, k0, na, nb; };
+
+// Next tile of the CTA's range from cursor (a, k0); atoms without pairs are skipped (and get G = 0
+// here when G is given).
+__device__ __forceinline__ bool next_tile_n6(const int* n6, float* G, int& a, int& k0, int i1, TileSeg& s, int t, int nt) {
+  while (a < i1 && __ldg(n6 + a) == 0) {
+    if (G)
+      for (int e = t; e < 256; e += nt) G[(size_t)a * 256 + e] = 0.f;
+    ++a;
+    k0 = 0;
+  }
+  if (a >= i1) return false;
+  const int rem = __ldg(n6 + a) - k0;
+  s.a = a; s.k0 = k0; s.na = min(rem, kTile); s.nb = 0;
+  if (s.na == rem) {
+    const int b = a + 1;
+    const int nbt = b < i1 ? __ldg(n6 + b) : 0;
+    if (s.na < kTile && nbt > 0) {
+      s.nb = min(nbt, kTile - s.na);
+      if (s.nb == nbt) { a = b + 1; k0 = 0; } else { a = b; k0 = s.nb; }
+    } else {
+      a += 1; k0 = 0;
+    }
+  } else {
+    k0 += s.na;
+  }
+  return true;
+}
+__device__ __forceinline__ bool next_tile(const DescArgs& d, int& a, int& k0, int i1, TileSeg& s, int t) {
+  return next_tile_n6(d.n6, d.G, a, k0, i1, s, t, 128);
+}
+
+// Row p of a tile: its atom, la, list entry and the two positions (loaded ahead of use).
+struct RowFetch {
+  int atom, la;
+  bool valid;
+  uint32_t ent;
+  float4 xi, xj;
+};
+__device__ __forceinline__ void fetch_entry(const DescArgs& d, const TileSeg& s, bool have, int p, RowFetch& f) {
+  f.valid = have && p < s.na + s.nb;
+  f.la = p < s.na ? 0 : 1;
+  f.atom = f.la ? s.a + 1 : s.a;
+  f.ent = 0;
+  if (f.valid) {
+    const int slot = f.la ? p - s.na : s.k0 + p;
+    f.ent = __ldg(d.list6 + (size_t)f.atom * d.cap6 + slot);
+    f.xi = __ldg(d.pos + f.atom);
+  }
+}
+__device__ __forceinline__ void fetch_xj(const DescArgs& d, RowFetch& f) {
+  if (f.valid) {
+    const int j = f.ent & NNPE_J_MASK;
+    f.xj = __ldg(d.pos + (j < d.npos ? j : 0));
+  }
+}
+
+struct DescRow {
+  float cs;     // scale * cff(r), 0 for rows past the tile's pairs
+  int tj, s, la;
+  bool valid;
+};
+
+// First layer of one row into A (block of species tj, zeros in the other block); returns the
+// row's epilogue data.
+__device__ __forceinline__ DescRow desc_first_layer(const DescArgs& d, const RowFetch& f, const float* sE,
+                                                    unsigned char* A, int p) {
+  DescRow r;
+  r.valid = f.valid; r.cs = 0.f; r.tj = 0; r.s = 0; r.la = f.la;
+  if (!f.valid) return r;
+  const float dx = f.xi.x - f.xj.x, dy = f.xi.y - f.xj.y, dz = f.xi.z - f.xj.z;
+  const float rr = sqrtf(dx * dx + dy * dy + dz * dz);
+  const float cf = rr - d.rc, den = 1.f + cf * cf;
+  r.cs = d.scale * (1.f - 1.f / den);
+  r.s = f.ent >> 30;
+  r.tj = (f.ent >> 27) & 7;
+  const float u = rr / d.rc;
+  const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
+  const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {   // 8 units per 16-byte chunk, tanh on BF16 pairs (h is a BF16 operand)
+    const float4 w0 = W1[2 * g], w1 = W1[2 * g + 1], b0 = B1[2 * g], b1 = B1[2 * g + 1];
+    uint4 h;
+    h.x = tanh_bf2(pack_bf2(fmaf(w0.x, u, b0.x), fmaf(w0.y, u, b0.y)));
+    h.y = tanh_bf2(pack_bf2(fmaf(w0.z, u, b0.z), fmaf(w0.w, u, b0.w)));
+    h.z = tanh_bf2(pack_bf2(fmaf(w1.x, u, b1.x), fmaf(w1.y, u, b1.y)));
+    h.w = tanh_bf2(pack_bf2(fmaf(w1.z, u, b1.z), fmaf(w1.w, u, b1.w)));
+    *reinterpret_cast<uint4*>(A + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = h;
+    *reinterpret_cast<uint4*>(A + tc::kmajor_off(p, 32 * (1 - r.tj) + 8 * g, kK64)) = make_uint4(0, 0, 0, 0);
+  }
+  return r;
+}
+
+// Warp 0: G rows (la, s) = lanes 4 la + s of the MMA 2 accumulator at taddr, added to the carried
+// partial of a segment that began in an earlier tile; stored when the atom's last pair was in this
+// tile, else carried.
+__device__ __forceinline__ void desc_readout(const DescArgs& d, uint32_t taddr, const TileSeg& sg, float* sCarry, int lane) {
+  float g[64];
+#pragma unroll
+  for (int c0 = 0; c0 < 64; c0 += 32) tc::tmem_ld16x2(taddr + c0, taddr + c0 + 16, g + c0, g + c0 + 16);
+  const int la = lane >> 2, sc = lane & 3;
+  const bool mine = lane < 8 && (la == 0 || sg.nb > 0);
+  const int atom = sg.a + la;
+  const int nrow = la ? sg.nb : sg.na, start = la ? 0 : sg.k0;
+  const bool done = mine && start + nrow == __ldg(d.n6 + atom);
+  if (mine && la == 0 && start > 0) {
+#pragma unroll
+    for (int c = 0; c < 64; ++c) g[c] += sCarry[sc * 64 + c];
+  }
+  __syncwarp();
+  if (mine) {
+    if (done) {
+      float4* dst = reinterpret_cast<float4*>(d.G + (size_t)atom * 256 + sc * 64);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) dst[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 64; ++c) sCarry[sc * 64 + c] = g[c];
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(128, 3) k_tc_desc2(DescArgs d) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ uint64_t bar_z[2], bar_g;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_range[2];
+  unsigned char* sW = sm;                                       // B of MMA 1 (64 x 64)
+  unsigned char* sA = sW + 64 * kK64 * 2;                       // 3 x [128 x 64]: H of MMA 1, then Y of MMA 2
+  unsigned char* sS = sA + kDescStages * kTile * kK64 * 2;      // A of MMA 2 (8 x 128)
+  float* sE = reinterpret_cast<float*>(sS + 8 * kTile * 2);     // per species W1 b1 b2 (stride 132)
+  float* sCarry = sE + 2 * kEmbStride4;                         // partial G of a segment cut by a tile end
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31, p = t;
+  if (w == 0) tc::tmem_alloc(&tmem_base, 128);
+  if (t == 0) {
+    tc::mbar_init(&bar_z[0], 1);
+    tc::mbar_init(&bar_z[1], 1);
+    tc::mbar_init(&bar_g, 1);
+    // atom range of this CTA (equal atom counts; the tiles below adapt to the pair counts)
+    int r[2];
+    for (int e = 0; e < 2; ++e) r[e] = (int)((long long)d.N * (blockIdx.x + e) / gridDim.x);
+    s_range[0] = r[0];
+    s_range[1] = r[1];
+  }
+  copy_image(sW, d.wdesc, 64 * kK64 * 2, t, 128);
+  for (int k = t; k < 2 * 128; k += 128) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < d.ntype ? d.emb_small[k] : 0.f;
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tmem_base;
+  const uint32_t lane_off = (uint32_t)(w * 32) << 16;
+  const uint32_t aW = tc::smem_u32(sW), aS = tc::smem_u32(sS);
+  const int i1 = s_range[1];
+  int ca = s_range[0], ck0 = 0;
+  uint32_t ph_z[2] = {0, 0}, ph_g = 0;
+  bool alive = true;
+
+  // prologue: tile 0 built, its MMA 1 issued; tile 1 fetched
+  TileSeg seg0{0, 0, 0, 0}, seg1{0, 0, 0, 0}, seg2{0, 0, 0, 0}, segp{0, 0, 0, 0};
+  bool have0 = next_tile(d, ca, ck0, i1, seg0, t);
+  RowFetch f0, f1, f2;
+  fetch_entry(d, seg0, have0, p, f0);
+  fetch_xj(d, f0);
+  bool have1 = have0 && next_tile(d, ca, ck0, i1, seg1, t);
+  fetch_entry(d, seg1, have1, p, f1);
+  DescRow row0 = desc_first_layer(d, f0, sE, sA, p);
+  fetch_xj(d, f1);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (have0 && t == 0) {
+    const uint32_t id = tc::idesc_bf16(128, 64);
+    for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(tc::smem_u32(sA), kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+    tc::mma_commit(&bar_z[0]);
+  }
+  bool havep = false;
+  int last_buf = 0;
+  DescRow row1 = row0;
+  for (int it = 0; have0 && alive; ++it) {
+    const int b0 = it & 1, b1 = b0 ^ 1;
+    unsigned char* A0 = sA + (size_t)(it % 3) * kTile * kK64 * 2;
+    unsigned char* A1 = sA + (size_t)((it + 1) % 3) * kTile * kK64 * 2;
+    // (1) first layer of tile it+1; loads of tile it+2
+    bool have2 = false;
+    seg2 = TileSeg{0, 0, 0, 0};
+    if (have1) {
+      row1 = desc_first_layer(d, f1, sE, A1, p);
+      have2 = next_tile(d, ca, ck0, i1, seg2, t);
+    }
+    fetch_entry(d, seg2, have2, p, f2);
+    // (2) one barrier: A[it+1] written; MMA 1 of tile it and MMA 2 of tile it-1 complete
+    tc::fence_async_smem();
+    tc::fence_before();
+    {
+      bool ok = true;
+      if (t == 0) {
+        ok = tc::mbar_wait(&bar_z[b0], ph_z[b0]) && (!havep || tc::mbar_wait(&bar_g, ph_g));
+        if (!ok) atomicOr(d.ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
+      }
+      alive = __syncthreads_and(ok) != 0;
+    }
+    tc::fence_after();
+    ph_z[b0] ^= 1;
+    if (havep) ph_g ^= 1;
+    if (!alive) break;
+    // (3) warp 0: G of tile it-1 out of TMEM[b1], then MMA 1 of tile it+1 into it
+    if (w == 0) {
+      if (havep) desc_readout(d, tmem + 64 * b1, segp, sCarry, lane);
+      if (have1 && lane == 0) {
+        tc::fence_after();
+        const uint32_t id = tc::idesc_bf16(128, 64);
+        const uint32_t aA = tc::smem_u32(A1);
+        for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem + 64 * b1, tc::tile_desc(aA, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+        tc::mma_commit(&bar_z[b1]);
+      }
+    }
+    // (4) epilogue of tile it: y = scale cff tanh(z + b2), on BF16 pairs (Y is a BF16 operand)
+    const int nrows = seg0.na + seg0.nb, NK = (nrows + 15) & ~15;
+    if (32 * w < NK) {   // warp-uniform
+      const float4* b2 = reinterpret_cast<const float4*>(sE + row0.tj * kEmbStride4 + 64);
+      const float csv = row0.valid ? row0.cs : 0.f;
+      const uint32_t cs2 = pack_bf2(csv, csv);
+#pragma unroll
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        float z[32];
+        tc::tmem_ld16x2(tmem + 64 * b0 + lane_off + c0, tmem + 64 * b0 + lane_off + c0 + 16, z, z + 16);
+        uint32_t y[16];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 bb = b2[(c0 >> 2) + q];
+          y[2 * q] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q] + bb.x, z[4 * q + 1] + bb.y)), cs2);
+          y[2 * q + 1] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q + 2] + bb.z, z[4 * q + 3] + bb.w)), cs2);
+        }
+        if (p < NK) {   // rows past the tile's pairs are exact zeros (their Z may be anything)
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4*>(A0 + tc::mnmajor_off(c0 + 8 * q, p, 64)) =
+                row0.valid ? make_uint4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]) : make_uint4(0, 0, 0, 0);
+        }
+      }
+      if (p < NK) {
+        const int m = 4 * row0.la + row0.s;
+        const uint16_t one = 0x3F80u;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          *reinterpret_cast<uint16_t*>(sS + tc::kmajor_off(c, p, kTile)) = (row0.valid && m == c) ? one : (uint16_t)0;
+      }
+    }
+    fetch_xj(d, f2);
+    // (5) MMA 2 of tile it
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (t == 0) {
+      const uint32_t id = tc::idesc_bf16(128, 64, true);
+      const uint32_t aY = tc::smem_u32(A0);
+      for (int kk = 0; kk < NK / 16; ++kk)
+        tc::mma_bf16(tmem + 64 * b0, tc::tile_desc_bcast(aS, kTile, kk), tc::tile_desc_mn(aY, 64, kk), id, kk > 0);
+      tc::mma_commit(&bar_g);
+    }
+    segp = seg0; havep = true; last_buf = b0;
+    seg0 = seg1; have0 = have1; row0 = row1;
+    seg1 = seg2; have1 = have2; f1 = f2;
+  }
+  // G of the last tile
+  if (havep && alive) {
+    alive = cta_wait_mma(&bar_g, ph_g, d.ctrl);
+    if (alive && w == 0) desc_readout(d, tmem + 64 * last_buf, segp, sCarry, lane);
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (w == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+// -------------------------------------------------------------------------------------------
 // Force. The pair (i, j) enters G_i through the net of t_j and G_j through the net of t_i, so
 // dE/dr_ij = T(i->j) + T(j->i) with T(i->j) = scale sum_c dE/dG_i[s*64+c] d(y_c cff)/dr, y the
 // net of t_j. Each directed pair of the full list computes its own T from the centre's dE/dG_i
@@ -482,6 +818,248 @@ __global__ void __launch_bounds__(256, 4) k_tc_force(TcArgs a) {
   if (w == 0) tc::tmem_dealloc(tmem, 128);
 }
 
+// -------------------------------------------------------------------------------------------
+// Force, pipelined over the packed tiles of the descriptor kernel (up to two atom segments per
+// tile). 256 threads: row p = t % 128, half h = t / 128 takes hidden units [16h, 16h+16) of the
+// first layer and channels [32h, 32h+32) of the epilogue (warps w and w+4 read the same TMEM
+// lanes). Per tile t:
+//   (1) first layer of tile t+1: H and V = dH/dr into A stage (t+1) % 2, dE/dG of its atoms into
+//       shared memory; loads of tile t+2 issued,
+//   (2) barrier, after which MMA of tile t is complete,
+//   (3) MMA of tile t+1: Z = H W2s and K = V W2s into TMEM stage (t+1) % 2 (128 columns),
+//   (4) epilogue of tile t: each half's share of T = scale (dcff sum_c a_c y_c + cff sum_c a_c
+//       kappa_c (1 - y_c^2)), y = tanh(z + b2), a = dE/dG_i[s*64 + c],
+//   (5) barrier; half 0: fpair = -T/r applied to j's owner (64-bit fixed-point atomics) and summed
+//       per atom segment over each warp (one atomic per segment and warp) for i; the virial the same.
+constexpr int kSmemForce2 = 64 * kK64 * 2 + 2 * 2 * kTile * kK64 * 2 + 2 * 2 * 256 * 4 + 2 * kEmbStride4 * 4 + 2 * kTile * 4;
+
+struct ForceArgs {
+  const float4* pos;
+  const uint32_t* list6;
+  const int* n6;
+  const int* gowner;
+  const unsigned char* wdesc;
+  const float* emb_small;
+  const float* dG;
+  unsigned long long* facc;   // [N][4]: force x, y, z and virial, fixed point (2^-32)
+  int* ctrl;
+  int cap6, N, ntype, npos;
+  float rc, scale;
+};
+
+struct ForceRow {
+  float dx, dy, dz, r, rsq, cff, dcff;
+  int s, tj, la, jo;
+  bool valid;
+};
+
+__device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const RowFetch& f, const float* sE,
+                                                      unsigned char* AH, unsigned char* AV, int p, int half) {
+  ForceRow r;
+  r.valid = f.valid; r.la = f.la; r.s = 0; r.tj = 0; r.jo = 0;
+  r.dx = r.dy = r.dz = 0.f; r.r = 1.f; r.rsq = 1.f; r.cff = 0.f; r.dcff = 0.f;
+  if (!f.valid) return r;
+  r.dx = f.xi.x - f.xj.x; r.dy = f.xi.y - f.xj.y; r.dz = f.xi.z - f.xj.z;
+  r.rsq = r.dx * r.dx + r.dy * r.dy + r.dz * r.dz;
+  r.r = sqrtf(r.rsq);
+  const float cf = r.r - a.rc, den = 1.f + cf * cf;
+  r.cff = 1.f - 1.f / den;
+  r.dcff = 2.f * cf / (den * den);
+  r.s = f.ent >> 30;
+  r.tj = (f.ent >> 27) & 7;
+  const int j = f.ent & NNPE_J_MASK;
+  r.jo = j < a.N ? j : __ldg(a.gowner + (j - a.N));
+  const float r_rc = 1.f / a.rc, u = r.r * r_rc;
+  const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
+  const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
+#pragma unroll
+  for (int gg = 0; gg < 2; ++gg) {
+    const int g = 2 * half + gg;   // 8-unit chunk
+    const float4 w0 = W1[2 * g], w1 = W1[2 * g + 1], b0 = B1[2 * g], b1 = B1[2 * g + 1];
+    const float w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    float h[8], v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      h[q] = tanh_fast(fmaf(w[q], u, bb[q]));
+      v[q] = (1.f - h[q] * h[q]) * w[q] * r_rc;
+    }
+    *reinterpret_cast<uint4*>(AH + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = tc::pack8(h);
+    *reinterpret_cast<uint4*>(AV + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = tc::pack8(v);
+    *reinterpret_cast<uint4*>(AH + tc::kmajor_off(p, 32 * (1 - r.tj) + 8 * g, kK64)) = make_uint4(0, 0, 0, 0);
+    *reinterpret_cast<uint4*>(AV + tc::kmajor_off(p, 32 * (1 - r.tj) + 8 * g, kK64)) = make_uint4(0, 0, 0, 0);
+  }
+  return r;
+}
+
+// dE/dG of the tile's atoms (1 or 2) into sdG[2][256].
+__device__ __forceinline__ void load_tile_dG(const ForceArgs& a, const TileSeg& sg, bool have, float* sdG, int t) {
+  if (!have) return;
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int k = t + 256 * e, la = k >> 8;
+    if (la == 0 || sg.nb > 0) sdG[k] = __ldg(a.dG + (size_t)(sg.a + la) * 256 + (k & 255));
+  }
+}
+
+__device__ __forceinline__ float seg_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool EV>
+__global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  unsigned char* sW = sm;                                          // 64 x 64
+  unsigned char* sAH = sW + 64 * kK64 * 2;                         // 2 stages x [H | V], 32 KB each
+  float* sdG = reinterpret_cast<float*>(sAH + 2 * 2 * kTile * kK64 * 2);   // 2 stages x [2][256]
+  float* sE = sdG + 2 * 512;
+  float* sAcc = sE + 2 * kEmbStride4;                              // [2][128] per-half partial T
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31, p = t & 127, half = t >> 7;
+  if (w == 0) tc::tmem_alloc(&tmem_base, 256);
+  if (t == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
+  copy_image(sW, a.wdesc, 64 * kK64 * 2, t, 256);
+  for (int k = t; k < 2 * 128; k += 256) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < a.ntype ? a.emb_small[k] : 0.f;
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tmem_base;
+  const uint32_t lane_off = (uint32_t)((w & 3) * 32) << 16;
+  const uint32_t aW = tc::smem_u32(sW);
+  const int i0 = (int)((long long)a.N * blockIdx.x / gridDim.x), i1 = (int)((long long)a.N * (blockIdx.x + 1) / gridDim.x);
+  int ca = i0, ck0 = 0;
+  uint32_t ph[2] = {0, 0};
+  bool alive = true;
+  // RowFetch reads list6/pos through a DescArgs view of the same arrays
+  DescArgs dv;
+  dv.pos = a.pos; dv.list6 = a.list6; dv.n6 = a.n6; dv.gowner = a.gowner; dv.cap6 = a.cap6; dv.N = a.N; dv.npos = a.npos;
+  TileSeg seg0{0, 0, 0, 0}, seg1{0, 0, 0, 0}, seg2{0, 0, 0, 0};
+  RowFetch f0, f1, f2;
+  bool have0 = next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg0, t, 256);
+  fetch_entry(dv, seg0, have0, p, f0);
+  fetch_xj(dv, f0);
+  bool have1 = have0 && next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg1, t, 256);
+  fetch_entry(dv, seg1, have1, p, f1);
+  ForceRow row0 = force_first_layer(a, f0, sE, sAH, sAH + kTile * kK64 * 2, p, half);
+  load_tile_dG(a, seg0, have0, sdG, t);
+  fetch_xj(dv, f1);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (have0 && t == 0) {
+    const uint32_t id = tc::idesc_bf16(128, 64);
+    const uint32_t aH = tc::smem_u32(sAH), aV = aH + kTile * kK64 * 2;
+    for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(aH, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+    for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem + 64, tc::tile_desc(aV, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+    tc::mma_commit(&bar[0]);
+  }
+  ForceRow row1 = row0;
+  for (int it = 0; have0 && alive; ++it) {
+    const int b0 = it & 1, b1 = b0 ^ 1;
+    unsigned char* AH1 = sAH + (size_t)b1 * 2 * kTile * kK64 * 2;
+    // (1) first layer and dE/dG of tile it+1; loads of tile it+2
+    bool have2 = false;
+    seg2 = TileSeg{0, 0, 0, 0};
+    if (have1) {
+      row1 = force_first_layer(a, f1, sE, AH1, AH1 + kTile * kK64 * 2, p, half);
+      load_tile_dG(a, seg1, true, sdG + 512 * b1, t);
+      have2 = next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg2, t, 256);
+    }
+    fetch_entry(dv, seg2, have2, p, f2);
+    // (2) barrier: MMA of tile it complete, stage it+1 written
+    tc::fence_async_smem();
+    tc::fence_before();
+    {
+      bool ok = true;
+      if (t == 0) {
+        ok = tc::mbar_wait(&bar[b0], ph[b0]);
+        if (!ok) atomicOr(a.ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
+      }
+      alive = __syncthreads_and(ok) != 0;
+    }
+    tc::fence_after();
+    ph[b0] ^= 1;
+    if (!alive) break;
+    // (3) MMA of tile it+1
+    if (have1 && t == 0) {
+      const uint32_t id = tc::idesc_bf16(128, 64);
+      const uint32_t aH = tc::smem_u32(AH1), aV = aH + kTile * kK64 * 2;
+      const uint32_t td = tmem + 128 * b1;
+      for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(td, tc::tile_desc(aH, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+      for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(td + 64, tc::tile_desc(aV, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+      tc::mma_commit(&bar[b1]);
+    }
+    // (4) epilogue of tile it: this half's share of T
+    const int nrows = seg0.na + seg0.nb;
+    float part = 0.f;
+    if (32 * (w & 3) < nrows) {   // warp-uniform: the loads below are warp-collective
+      const float* ag = sdG + 512 * b0 + row0.la * 256 + row0.s * 64 + 32 * half;
+      const float* b2 = sE + row0.tj * kEmbStride4 + 64 + 32 * half;
+      float sy = 0.f, sk = 0.f;
+#pragma unroll
+      for (int c0 = 0; c0 < 32; c0 += 16) {
+        float z[16], kap[16];
+        tc::tmem_ld16x2(tmem + 128 * b0 + lane_off + 32 * half + c0, tmem + 128 * b0 + lane_off + 64 + 32 * half + c0, z, kap);
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) {
+          const float4 a4 = *reinterpret_cast<const float4*>(ag + c0 + q);
+          const float4 bb = *reinterpret_cast<const float4*>(b2 + c0 + q);
+          const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {bb.x, bb.y, bb.z, bb.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float y = tanh_fast(z[q + e] + bv[e]);
+            sy = fmaf(av[e], y, sy);
+            sk = fmaf(av[e] * kap[q + e], fmaf(-y, y, 1.f), sk);
+          }
+        }
+      }
+      if (row0.valid) part = a.scale * (row0.dcff * sy + row0.cff * sk);
+    }
+    sAcc[half * kTile + p] = part;
+    fetch_xj(dv, f2);
+    __syncthreads();
+    // (5) half 0: pair forces to j's owner, per-segment sums for the atoms of the tile
+    if (half == 0) {
+      float gx = 0.f, gy = 0.f, gz = 0.f, vr = 0.f;
+      if (row0.valid) {
+        const float fpair = -(sAcc[p] + sAcc[kTile + p]) / row0.r;
+        gx = row0.dx * fpair; gy = row0.dy * fpair; gz = row0.dz * fpair;
+        if (EV) vr = fpair * row0.rsq;
+        unsigned long long* fj = a.facc + 4 * (size_t)row0.jo;
+        fix_add(fj, -gx); fix_add(fj + 1, -gy); fix_add(fj + 2, -gz);
+      }
+      const unsigned in0 = __ballot_sync(0xffffffffu, row0.valid && row0.la == 0);
+      const unsigned in1 = __ballot_sync(0xffffffffu, row0.valid && row0.la == 1);
+#pragma unroll
+      for (int sgm = 0; sgm < 2; ++sgm) {
+        const unsigned in = sgm ? in1 : in0;
+        if (!in) continue;   // warp-uniform
+        const bool mine = row0.valid && row0.la == sgm;
+        const float sx = seg_sum(mine ? gx : 0.f), sy2 = seg_sum(mine ? gy : 0.f), sz = seg_sum(mine ? gz : 0.f);
+        const float sv = EV ? seg_sum(mine ? vr : 0.f) : 0.f;
+        if (lane == 0) {
+          unsigned long long* fi = a.facc + 4 * (size_t)(seg0.a + sgm);
+          fix_add(fi, sx); fix_add(fi + 1, sy2); fix_add(fi + 2, sz);
+          if (EV) fix_add(fi + 3, sv);
+        }
+      }
+    }
+    seg0 = seg1; have0 = have1; row0 = row1;
+    seg1 = seg2; have1 = have2; f1 = f2;
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (w == 0) tc::tmem_dealloc(tmem, 256);
+}
+
 // frc[i] += fixed-point network force of atom i
 __global__ void k_facc_apply(const unsigned long long* __restrict__ facc, float4* __restrict__ frc, int N) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -492,6 +1070,20 @@ __global__ void k_facc_apply(const unsigned long long* __restrict__ facc, float4
   f.y += (float)((double)(long long)facc[3 * i + 1] * s);
   f.z += (float)((double)(long long)facc[3 * i + 2] * s);
   frc[i] = f;
+}
+
+// frc[i] += network force of atom i, watom[i] += its virial (EV), from the [N][4] fixed-point sums.
+template <bool EV>
+__global__ void k_facc_apply4(const unsigned long long* __restrict__ facc, float4* __restrict__ frc, double* watom, int N) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double s = 1.0 / kFix;
+  float4 f = frc[i];
+  f.x += (float)((double)(long long)facc[4 * i] * s);
+  f.y += (float)((double)(long long)facc[4 * i + 1] * s);
+  f.z += (float)((double)(long long)facc[4 * i + 2] * s);
+  frc[i] = f;
+  if (EV) watom[i] += (double)(long long)facc[4 * i + 3] * s;
 }
 
 // -------------------------------------------------------------------------------------------
@@ -529,13 +1121,22 @@ __device__ __forceinline__ void sync_image(unsigned char* sW, const unsigned cha
   copy_image(sW, src, bytes, t, 128);
 }
 
+// Weight image -> shared memory with cp.async (16 B per copy), one commit group per call.
+__device__ __forceinline__ void prefetch_image(unsigned char* dst, const unsigned char* src, int bytes, int t, int nt) {
+  for (int k = t; k < bytes / 16; k += nt) tc::cp_async16(dst + 16 * k, src + 16 * k);
+  tc::cp_async_commit();
+}
+
+// 128 atoms of one species per CTA; the four weight images stream through two shared buffers so
+// that each image's copy overlaps the MMA chain and epilogue before it.
 __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
   unsigned char* sAct = sm;                 // 128 x 256 (G), later 128 x 128 (g2)
   unsigned char* sH1 = sm + 128 * 256 * 2;  // 128 x 128 (h1, later g1)
-  unsigned char* sW = sH1 + 128 * 128 * 2;  // up to 64 KB
+  unsigned char* sW0 = sH1 + 128 * 128 * 2; // L1, then B2
+  unsigned char* sW1 = sW0 + 128 * 256 * 2; // L2, then B1
   const int t = threadIdx.x, w = t >> 5;
   const int sp = f.tile_sp[blockIdx.x], row0 = f.tile_row[blockIdx.x];
   const int M = f.soff[sp + 1] - f.soff[sp];
@@ -546,6 +1147,8 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
   const float *sm_c2 = sm_c1 + 128, *sm_a3 = sm_c1 + 256, *sm_c3 = sm_c1 + 384;
   if (w == 0) tc::tmem_alloc(&tmem_base, 256);
   if (t == 0) tc::mbar_init(&bar, 1);
+  prefetch_image(sW0, img, (int)kImgL1, t, 128);                    // group: L1
+  prefetch_image(sW1, img + kImgL1, (int)kImgL2, t, 128);           // group: L2
   // G row -> bf16 A tile (K=256)
   for (int k = 0; k < 256; k += 8) {
     float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -556,13 +1159,14 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
     }
     *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(t, k, 256)) = tc::pack8(g);
   }
-  copy_image(sW, img, (int)kImgL1, t, 128);
+  tc::cp_async_wait<1>();   // L1 landed
   const uint32_t tmem = tmem_base;
   const uint32_t taddr = tmem + ((uint32_t)(w * 32) << 16);
-  const uint32_t aAct = tc::smem_u32(sAct), aH1 = tc::smem_u32(sH1), aW = tc::smem_u32(sW);
+  const uint32_t aAct = tc::smem_u32(sAct), aH1 = tc::smem_u32(sH1), aW0 = tc::smem_u32(sW0), aW1 = tc::smem_u32(sW1);
   bool ok = true;
   // L1: z1 = G A1 (+c1), h1 = tanh
-  ok = fit_mma(tmem, aAct, 256, aW, 128, &bar, 0, t, f.ctrl);
+  ok = fit_mma(tmem, aAct, 256, aW0, 128, &bar, 0, t, f.ctrl);
+  prefetch_image(sW0, img + kImgL1 + kImgL2, (int)kImgB2, t, 128);   // group: B2 (L1 consumed)
   if (ok) {
     for (int c0 = 0; c0 < 128; c0 += 16) {
       float v[16];
@@ -573,9 +1177,10 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
       *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(t, c0 + 8, 128)) = tc::pack8(v + 8);
     }
   }
-  sync_image(sW, img + kImgL1, (int)kImgL2, t);
+  tc::cp_async_wait<1>();   // L2 landed
   // L2: z2 = h1 A2 (+c2), h2 = tanh, E = h2 A3 + c3, g2 = A3 (1-h2^2)
-  if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW, 128, &bar, 1, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW1, 128, &bar, 1, t, f.ctrl);
+  prefetch_image(sW1, img + kImgL1 + kImgL2 + kImgB2, (int)kImgB1, t, 128);   // group: B1 (L2 consumed)
   if (ok) {
     float e = 0.f;
     for (int c0 = 0; c0 < 128; c0 += 16) {
@@ -592,9 +1197,9 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
     }
     if (valid) f.enet[atom] = (double)e + (double)sm_c3[0];
   }
-  sync_image(sW, img + kImgL1 + kImgL2, (int)kImgB2, t);
+  tc::cp_async_wait<1>();   // B2 landed
   // B2: u = g2 A2^T, g1 = u (1-h1^2)
-  if (ok) ok = fit_mma(tmem, aAct, 128, aW, 128, &bar, 0, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem, aAct, 128, aW0, 128, &bar, 0, t, f.ctrl);
   if (ok) {
     for (int c0 = 0; c0 < 128; c0 += 16) {
       float v[16];
@@ -615,9 +1220,9 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
       }
     }
   }
-  sync_image(sW, img + kImgL1 + kImgL2 + kImgB2, (int)kImgB1, t);
+  tc::cp_async_wait<0>();   // B1 landed
   // B1: dE/dG = g1 A1^T (N = 256)
-  if (ok) ok = fit_mma(tmem, aH1, 128, aW, 256, &bar, 1, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem, aH1, 128, aW1, 256, &bar, 1, t, f.ctrl);
   if (ok) {
     for (int c0 = 0; c0 < 256; c0 += 16) {
       float v[16];
@@ -629,6 +1234,7 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
       }
     }
   }
+  tc::cp_async_wait<0>();
   tc::fence_before();
   __syncthreads();
   if (w == 0) tc::tmem_dealloc(tmem, 256);
@@ -655,7 +1261,7 @@ void put_image(std::vector<uint16_t>& img, size_t base, int N, int K, F&& val) {
 void nnp_tc_free(NnpModel* m) {
   NnpTc* t = m->tc;
   if (!t) return;
-  for (void* p : {(void*)t->d_wdesc, (void*)t->d_facc, (void*)t->d_fit, (void*)t->d_emb_small, (void*)t->d_fit_small,
+  for (void* p : {(void*)t->d_wdesc64, (void*)t->d_wdesc, (void*)t->d_facc, (void*)t->d_fit, (void*)t->d_emb_small, (void*)t->d_fit_small,
                   (void*)t->d_tile_sp, (void*)t->d_tile_row, (void*)t->d_soff})
     if (p) dev_free(p);
   delete t;
@@ -678,6 +1284,8 @@ int nnp_tc_setup(nnpe_ctx* c) {
     if (k < 64) return k / 32 < T ? E[eb * (k / 32) + 64 + (k % 32) * 64 + n] : 0.f;
     return k - 64 < T ? E[eb * (k - 64) + 64 + 32 * 64 + n] : 0.f;   // bias rows b2_t
   });
+  std::vector<uint16_t> wdesc64((size_t)64 * kK64);
+  put_image(wdesc64, 0, 64, kK64, [&](int n, int k) { return k / 32 < T ? E[eb * (k / 32) + 64 + (k % 32) * 64 + n] : 0.f; });
   std::vector<float> emb_small((size_t)T * 128);
   for (int s = 0; s < T; ++s)
     for (int q = 0; q < 32; ++q) {
@@ -716,7 +1324,8 @@ int nnp_tc_setup(nnpe_ctx* c) {
     return 0;
   };
   if (int rc = up((void**)&t->d_wdesc, wdesc.data(), wdesc.size() * 2)) return rc;
-  NNPE_CUDA(c, dev_malloc(c, (void**)&t->d_facc, sizeof(unsigned long long) * 3 * std::max(c->natom, 1)));
+  if (int rc = up((void**)&t->d_wdesc64, wdesc64.data(), wdesc64.size() * 2)) return rc;
+  NNPE_CUDA(c, dev_malloc(c, (void**)&t->d_facc, sizeof(unsigned long long) * 4 * std::max(c->natom, 1)));
   if (int rc = up((void**)&t->d_fit, fit.data(), fit.size() * 2)) return rc;
   if (int rc = up((void**)&t->d_emb_small, emb_small.data(), emb_small.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_fit_small, fit_small.data(), fit_small.size() * 4)) return rc;
@@ -724,17 +1333,14 @@ int nnp_tc_setup(nnpe_ctx* c) {
   if (int rc = up((void**)&t->d_tile_row, trow.data(), trow.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_soff, m->soff.data(), m->soff.size() * 4)) return rc;
   const int smem_desc = kSmemDesc, smem_force = kSmemForce;
-  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 256 * 128 * 2;
+  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 2 * 256 * 128 * 2;
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_desc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_desc));
+  NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_desc2, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDesc2));
+  NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemForce2));
+  NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemForce2));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fit));
-  // one wave of resident CTAs: a grid larger than what fits leaves a partial second wave
-  int od = 0, of = 0;
-  NNPE_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, k_tc_desc, 128, smem_desc));
-  NNPE_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&of, k_tc_force<true>, 256, smem_force));
-  t->ctas_desc = std::max(1, std::min(od, 512 / 64));
-  t->ctas_force = std::max(1, std::min(of, 512 / 128));
   return 0;
 }
 
@@ -748,18 +1354,31 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   a.emb_small = t->d_emb_small; a.G = m->d_G; a.dG = m->d_dG; a.frc = c->d_frc; a.watom = c->d_watom; a.ctrl = c->d_ctrl;
   a.cap6 = m->cap6; a.N = c->natom; a.Kd = Kd; a.ntype = c->ntype; a.npos = c->natom + c->Gcap; a.rc = m->rc; a.scale = m->scale;
   const int sms = nnpe_sm_count(c->device);
-  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 256 * 128 * 2;
-  k_tc_desc<<<std::min(c->natom, sms * t->ctas_desc), 128, kSmemDesc, c->stream>>>(a);
+  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 2 * 256 * 128 * 2;
+  DescArgs dd;
+  dd.pos = c->d_pos; dd.list6 = m->d_list6; dd.n6 = m->d_n6; dd.gowner = c->d_gowner;
+  dd.wdesc = t->d_wdesc64; dd.emb_small = t->d_emb_small; dd.G = m->d_G; dd.ctrl = c->d_ctrl;
+  dd.cap6 = m->cap6; dd.N = c->natom; dd.ntype = c->ntype; dd.npos = c->natom + c->Gcap; dd.rc = m->rc; dd.scale = m->scale;
+  k_tc_desc2<<<std::max(1, std::min(c->natom, sms * t->ctas_desc)), 128, kSmemDesc2, c->stream>>>(dd);
   FitTcArgs f;
   f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row; f.G = m->d_G;
   f.fit = t->d_fit; f.fit_stride = t->fit_stride; f.small = t->d_fit_small; f.dG = m->d_dG; f.enet = m->d_enet;
   f.ctrl = c->d_ctrl;
   k_tc_fit<<<t->ntiles, 128, smem_fit, c->stream>>>(f);
-  NNPE_CUDA(c, cudaMemsetAsync(t->d_facc, 0, sizeof(unsigned long long) * 3 * c->natom, c->stream));
-  const int gforce = std::min(c->natom, sms * t->ctas_force);
-  if (ev) k_tc_force<true><<<gforce, 256, kSmemForce, c->stream>>>(a);
-  else k_tc_force<false><<<gforce, 256, kSmemForce, c->stream>>>(a);
-  k_facc_apply<<<(c->natom + 255) / 256, 256, 0, c->stream>>>(t->d_facc, c->d_frc, c->natom);
+  NNPE_CUDA(c, cudaMemsetAsync(t->d_facc, 0, sizeof(unsigned long long) * 4 * c->natom, c->stream));
+  ForceArgs fa;
+  fa.pos = c->d_pos; fa.list6 = m->d_list6; fa.n6 = m->d_n6; fa.gowner = c->d_gowner; fa.wdesc = t->d_wdesc64;
+  fa.emb_small = t->d_emb_small; fa.dG = m->d_dG; fa.facc = t->d_facc; fa.ctrl = c->d_ctrl;
+  fa.cap6 = m->cap6; fa.N = c->natom; fa.ntype = c->ntype; fa.npos = c->natom + c->Gcap; fa.rc = m->rc; fa.scale = m->scale;
+  const int gforce = std::max(1, std::min(c->natom, sms * t->ctas_force));
+  const int gapply = (c->natom + 255) / 256;
+  if (ev) {
+    k_tc_force2<true><<<gforce, 256, kSmemForce2, c->stream>>>(fa);
+    k_facc_apply4<true><<<gapply, 256, 0, c->stream>>>(t->d_facc, c->d_frc, c->d_watom, c->natom);
+  } else {
+    k_tc_force2<false><<<gforce, 256, kSmemForce2, c->stream>>>(fa);
+    k_facc_apply4<false><<<gapply, 256, 0, c->stream>>>(t->d_facc, c->d_frc, c->d_watom, c->natom);
+  }
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

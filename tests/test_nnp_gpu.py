@@ -148,3 +148,36 @@ def test_embed_nnp_bf16_md_steps():
         assert e.device_errors() == 0
     assert all(np.isfinite(r["erg"]) for r in logs[0][0])
     np.testing.assert_array_equal(logs[0][1], logs[1][1])
+
+
+@pytest.mark.parametrize("rho", [0.003, 0.2])
+def test_embed_nnp_bf16_sparse_and_dense_pair_counts(rho):
+    """The tensor-core kernels cut each CTA's pairs into tiles of up to two atom segments: a dilute
+    mixture (most atoms have no neighbour inside 6 A, tiles hold one or two short segments) and a
+    dense one (about 180 neighbours, an atom's pairs span two or three tiles) both reproduce the
+    FP64 oracle within the BF16 bar, and atoms without pairs get a zero descriptor."""
+    from nnpengine_b200 import systems as S
+    s = S.lj_mixture(600, rho, 0.6, seed=5)
+    m = NM.embed_model()
+    e = Engine(0)
+    e.set_system(s)
+    e.set_velocities(np.zeros_like(s.v))
+    e.setup(6.0, 2.0, 6.0, 2048)
+    e.pair_enable(False)
+    e.nnp_set(m, 6.0, 750)
+    e.nnp_precision(True)
+    e.list_build()
+    e.compute_forces(True)
+    assert e.device_errors() == 0
+    r, G, dG, ea = _bf16_vs_fp64(s, m, e)
+    lone = np.all(r["G"] == 0, axis=1)
+    if rho < 0.01:
+        assert lone.sum() > 100
+    else:
+        assert not lone.any()
+    assert np.all(G[lone] == 0)
+    assert cases.rel_rms(G, r["G"]) < 1e-2
+    assert cases.rel_rms(e.forces(), r["f"]) < 1e-2
+    e.compute_forces(True)   # deterministic
+    G2, _, _ = e.nnp_get()
+    np.testing.assert_array_equal(G, G2)
