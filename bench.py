@@ -43,6 +43,12 @@ WORKLOADS = {
     "water3k-classical": dict(n_side=10, bl=31.04, nmol=None, nnp=None,
                               desc="3,000-atom water (1,000 molecules, 31.04 A box), tabulated LJ + DSF Coulomb at 10 A, "
                                    "2 A skin, bonds + angles, dt 0.5 fs NVE"),
+    "gr-refine-30k": dict(mixture=True, natom=30000, rho=0.035, nnp=None,
+                          desc="g(r)/S(q) refinement: 30,000-atom two-species LJ + DSF Coulomb liquid (60/40, sigma "
+                               "3.0/3.4 A, eps 0.15/0.25 kcal/mol, charges +-0.5 e) at 0.035 A^-3 (94.99 A box); g(r) "
+                               "to 15 A in 0.01 A bins (uint64 counts) every step (cell-based every 10), S(q) on 512 "
+                               "points in FP64, RMDF (gamma 1) against the weighted S(q) of the same liquid with eps "
+                               "x1.1, Andersen 300 K, dt 1 fs"),
     "serve256": dict(serve=True, nnp="bf16",
                      desc="served replica stream: 256 seeded requests, water boxes of log-uniform 300-30,000 atoms at "
                           "0.95-1.05 g/cm^3 and 250-400 K (Andersen every 20 steps), 100-5000 steps each (uniform "
@@ -120,9 +126,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+MIX_SIGMA, MIX_EPS = (3.0, 3.4), (0.15, 0.25)
+
+
 def build_system(wl):
     import cases
     from nnpengine_b200 import systems as S
+    if wl.get("mixture"):
+        s = S.lj_mixture(wl["natom"], wl["rho"], 0.6, seed=4)
+        return s, S.lj_table(2, MIX_SIGMA, MIX_EPS, 10.0, 1000)
     s = S.water_box(wl["n_side"], wl["bl"], seed=2, nmol=wl.get("nmol"))
     r, F, U = S.water_lj_table(10.0, 1000)
     return s, (r, F, U)
@@ -135,9 +147,11 @@ def make_engine(s, table, device, nnp=None):
     F, U = cases.table_as_loaded(table[1], table[2])
     e = E.Engine(device)
     e.set_system(s)
-    e.setup(10.0, 2.0, 10.0, 1024)
+    mixture = s.moltypes[0].n_atom == 1
+    e.setup(10.0, 2.0, 15.0 if mixture else 10.0, 1024)
     e.set_pair_table(F, U)
-    e.set_bonded(s, [E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)], [E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)])
+    if not mixture:
+        e.set_bonded(s, [E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)], [E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)])
     if nnp:
         e.nnp_set(NM.embed_model(), 6.0, 750)
         e.nnp_precision(nnp == "bf16")
@@ -159,6 +173,14 @@ def cpu_reference(wl, steps: int):
                "bond": [f"1.0 {cases.WATER_BOND_K}"], "angle": [f"109.47 0 0 {cases.WATER_ANGLE_KC}"],
                "velocity": f["vel"], "mode": "md", "steps": steps, "dt": 0.5, "log_interval": steps}
         what = "LJ/DSF table + bonded"
+        if wl.get("mixture"):
+            from nnpengine_b200 import systems as S
+            q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, 2)
+            tpath = os.path.join(d, "sq_target.txt")
+            S.write_sq_target(tpath, q, sqex, wt, ff)
+            cfg.update({"gr_cutoff": 15, "nq": 512, "qmax": 20, "gr_interval": "1 10", "rmdf": f"0.02 1.0 {tpath}",
+                        "dt": 1.0})
+            what = "LJ/DSF table, g(r) every step (cell-based every 10), S(q) and RMDF"
         if wl.get("nnp"):
             paths = cases.write_nnp_inputs(NM.gauss_model(h1=128, h2=128), d)
             cfg["nnp"] = f"6.0 750 {paths['param']} {paths['wt']}"
@@ -235,6 +257,57 @@ def serve_bench(args, wl):
                 clocks=clk.summary(), wall_after_last_submit_s=t_end - t_arr[-1])
 
 
+def refine_setup(e, s, wl, device, args):
+    """RMDF target: the weighted S(q) of the same liquid with every eps scaled by 1.1 after
+    `--target-steps` steps at 300 K (Andersen), computed by the library itself; then g(r) every step
+    (cell-based every 10) and RMDF with gamma 1 on the workload's engine."""
+    from nnpengine_b200 import systems as S
+    r, F11, U11 = S.lj_table(2, MIX_SIGMA, tuple(1.1 * x for x in MIX_EPS), 10.0, 1000)
+    et = make_engine(s, (r, F11, U11), device)
+    et.verlet(1.0, True)
+    et.thermostat("andersen", 300.0, 300.0, interval=1, frac=0.1, seed=21, total_steps=0)
+    et.gr_setup(1000, 512, 20.0)
+    et.run(args.target_steps, log_interval=args.target_steps, graph=True)
+    et.gr_tally(inner=False)
+    et.sq(False)
+    q, _, wt, ff = S.synthetic_sq_target(512, 20.0, 2)
+    et.rmdf_set(np.zeros((1, 512)), wt[None], ff[None], 0.0, 1.0)
+    et.rmdf_step()
+    target = et.rmdf_get()[0][0].copy()
+    et.close()
+    e.gr_setup(1000, 512, 20.0, gr_interval=1, gr_interval_long=10)
+    e.rmdf_set(target[None], wt[None], ff[None], args.rmdf_strength, 1.0)
+    return target
+
+
+def nve_drift(e, natom, ps, dt=0.5):
+    """Total energy over `ps` picoseconds of NVE (FP64 energies on log steps): linear-fit slope and
+    largest excursion from the first value."""
+    nsteps = int(round(ps * 1000 / dt))
+    every = max(1, nsteps // 40)
+    lg = e.run(nsteps + 1, log_interval=every, graph=True)
+    t = np.array([r["step"] for r in lg], float)
+    t = (t - t[0]) * dt / 1000.0
+    etot = np.array([r["erg"] + r["ekin"] for r in lg])
+    slope = float(np.polyfit(t, etot, 1)[0]) if len(t) > 1 else 0.0
+    return {"ps": ps, "dt_fs": dt, "steps": nsteps, "log_points": len(lg), "etot_first": float(etot[0]),
+            "etot_last": float(etot[-1]), "max_abs_dev_kcal_mol": float(np.abs(etot - etot[0]).max()),
+            "slope_kcal_mol_per_ps": slope, "slope_kcal_mol_per_atom_per_ns": slope * 1000.0 / natom,
+            "ekin_mean_kcal_mol": float(np.mean([r["ekin"] for r in lg])),
+            "temperature_mean_k": float(np.mean([r["temperature"] for r in lg]))}
+
+
+def profile_traffic(kernel_names):
+    """DRAM bytes per launch of the named kernels from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p)).get("kernels", {})
+    if not all(k in d for k in kernel_names):
+        return None
+    return sum(d[k]["dram_bytes_per_launch"] for k in kernel_names)
+
+
 def time_enqueue(e, stream, which, reps):
     import torch
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -263,6 +336,9 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-scale", type=float, default=1.0, help="multiply every request's step count")
     ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--drift-ps", type=float, default=0.0, help="after the timed steps, NVE for this many ps")
+    ap.add_argument("--target-steps", type=int, default=500)
+    ap.add_argument("--rmdf-strength", type=float, default=0.02)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -320,6 +396,9 @@ def main():
     e = make_engine(s, table, local, wl.get("nnp"))
     e.pair_exact(args.exact)
     stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
+    refine = wl.get("mixture")
+    if refine:
+        refine_setup(e, s, wl, local, args)
     # untimed equilibration of the classical model from the lattice start (Andersen at 300 K,
     # dt 1 fs, the 5 ps of the workload's definition), then the network on and NVE at dt=0.5 fs
     e.verlet(1.0, True)
@@ -330,8 +409,11 @@ def main():
         e.run(args.equil, log_interval=args.equil, graph=True)
     if wl.get("nnp"):
         e.nnp_enable(True)
-    e.thermostat("none")
-    e.verlet(0.5, True)
+    if refine:   # the refinement runs under the thermostat at dt 1 fs, as the reference's classical mode
+        e.thermostat("andersen", 300.0, 300.0, interval=10, frac=0.1, seed=12, total_steps=0)
+    else:
+        e.thermostat("none")
+        e.verlet(0.5, True)
     wlog = e.run(args.warmup, log_interval=max(args.warmup, 1), graph=True)
     nbuild0 = wlog[-1]["nbuild"] if wlog else 0
 
@@ -342,7 +424,7 @@ def main():
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         t0.record(stream)
-        log = e.run(args.steps, log_interval=args.steps, graph=True)
+        log = e.run(args.steps, log_interval=max(1, args.steps // 10) if refine else args.steps, graph=True)
         t1.record(stream)
         torch.cuda.synchronize()
     if dist:
@@ -358,30 +440,12 @@ def main():
     value = s.natom * args.steps * world / (ms / 1e3)
     launches = int(e.lib.nnpe_launches_per_step(e.h))
 
-    # per-kernel-class device time (CUDA events on the library stream)
-    reps = 20
-    e.compute_forces(ev=False)
-    kms = {"pair": time_enqueue(e, stream, 0, reps), "bonded": time_enqueue(e, stream, 2, reps),
-           "verlet": time_enqueue(e, stream, 4, reps), "rebuild": time_enqueue(e, stream, 1, 5)}
-    if wl.get("nnp"):
-        kms["network"] = time_enqueue(e, stream, 3, reps)
-    hbm, bf16, bf16s, src = peaks()
-    nlist = info["entries"] / s.natom
-    if wl.get("nnp"):
-        # network pairs inside 6 A from the compact list of the last evaluation
-        G, dG, ea = e.nnp_get()
-        pairs6 = int(e.lib.nnpe_nnp_pairs(e.h))
-        flops = nnp_flops_per_step(s.natom, pairs6)
-        ach = flops / (kms["network"] / 1e3) / 1e12
-        roof = {"bound": "tensor", "kernel": "network (k_tc_desc + k_tc_fit + k_tc_force)" if wl["nnp"] == "bf16"
-                else "network (FP32 CUDA cores)", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
-                "traffic": None, "peak_source": src, "kernel_ms": kms["network"], "alg_flops_per_launch": flops,
-                "pairs_in_6A_per_atom": pairs6 / s.natom}
-    else:
-        alg_bytes = s.natom * (4 * nlist + 48)
-        ach = alg_bytes / (kms["pair"] / 1e3) / 1e9
-        roof = {"bound": "hbm", "kernel": "k_pair", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": None, "peak_source": src, "kernel_ms": kms["pair"], "alg_bytes_per_launch": alg_bytes}
+    # state of the timed run, the start of the host-buffer (e2e) steps below
+    x_e2e0, v_e2e0 = e.positions().astype(np.float32), e.velocities().astype(np.float32)
+
+    drift = None
+    if args.drift_ps > 0 and not refine:
+        drift = nve_drift(e, s.natom, args.drift_ps)
 
     plain = None
     if wl.get("nnp") == "bf16" and not args.no_compare:
@@ -397,14 +461,53 @@ def main():
         plain = s.natom * world / (a.elapsed_time(b) / nfp / 1e3)
         e.nnp_precision(True)
 
+    # per-kernel-class device time (CUDA events on the library stream); these launches change the
+    # dynamical state (forces accumulate, velocities advance), so they come after every run that
+    # evolves it
+    reps = 20
+    e.compute_forces(ev=False)
+    kms = {"pair": time_enqueue(e, stream, 0, reps), "bonded": time_enqueue(e, stream, 2, reps),
+           "verlet": time_enqueue(e, stream, 4, reps), "rebuild": time_enqueue(e, stream, 1, 5)}
+    if wl.get("nnp"):
+        kms["network"] = time_enqueue(e, stream, 3, reps)
+    hbm, bf16, bf16s, src = peaks()
+    nlist = info["entries"] / s.natom
+    if wl.get("nnp"):
+        # network pairs inside 6 A from the compact list of the last evaluation
+        G, dG, ea = e.nnp_get()
+        pairs6 = int(e.lib.nnpe_nnp_pairs(e.h))
+        flops = nnp_flops_per_step(s.natom, pairs6)
+        ach = flops / (kms["network"] / 1e3) / 1e12
+        tc_kernels = ["k_tc_desc2", "k_tc_fit", "k_tc_force2<0>"]
+        roof = {"bound": "tensor", "kernel": "network (k_tc_desc2 + k_tc_fit + k_tc_force2)" if wl["nnp"] == "bf16"
+                else "network (FP32 CUDA cores)", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
+                "traffic": profile_traffic(tc_kernels) if wl["nnp"] == "bf16" else None,
+                "traffic_unit": "bytes per launch (DRAM read+write, ncu)", "peak_source": src,
+                "kernel_ms": kms["network"], "alg_flops_per_launch": flops, "pairs_in_6A_per_atom": pairs6 / s.natom}
+    else:
+        alg_bytes = s.natom * (4 * nlist + 48)
+        ach = alg_bytes / (kms["pair"] / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_pair", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": profile_traffic([f"k_pair<0,0>:{args.workload}"]), "traffic_unit": "bytes per launch (DRAM read+write, ncu)",
+                "peak_source": src, "kernel_ms": kms["pair"], "alg_bytes_per_launch": alg_bytes}
+    gr_info = None
+    if refine:
+        kms["gr_cell"] = time_enqueue(e, stream, 5, 10)
+        kms["gr_list"] = time_enqueue(e, stream, 6, 10)
+        ordered = float(e.gr_counts(False).sum())
+        exp = [r["erg_exp"] for r in log]
+        gr_info = {"ordered_pairs_per_cell_tally": ordered,
+                   "cell_tally_pair_evaluations_per_s": ordered / (kms["gr_cell"] / 1e3),
+                   "rmdf_penalty_first_last": [exp[0], exp[-1]] if exp else None, "rmdf_strength": args.rmdf_strength,
+                   "target": "weighted S(q) of the eps x1.1 liquid after %d steps (library-computed)" % args.target_steps}
+
     e2e = None
     if not args.no_e2e:
         import ctypes as C
         n3 = s.natom * 3
         x_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
         f_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
-        x0 = e.positions().astype(np.float32)
-        v0 = e.velocities().astype(np.float32)
+        x0, v0 = x_e2e0, v_e2e0
         erg = C.c_double(0)
         e2e_steps = max(10, args.steps // 4)
         xs = [(x0 + np.float32(k * 0.5) * v0).ravel() for k in range(e2e_steps + 3)]
@@ -441,6 +544,10 @@ def main():
         if plain is not None:
             cfg["plain_fp32_value"] = plain
             cfg["bf16_over_fp32"] = value / plain
+        if gr_info is not None:
+            cfg["gr_refinement"] = gr_info
+        if drift is not None:
+            cfg["nve_drift"] = drift
         out = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
