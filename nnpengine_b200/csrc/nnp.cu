@@ -225,12 +225,22 @@ __global__ void __launch_bounds__(128) k_filter6(const float4* __restrict__ pos,
 }
 
 // Species membership lists (sorted atom indices grouped by type) for the per-species fitting net.
+// (The order within a species is arbitrary: every fitting row depends on its own atom only.)
+// One counter update per warp and species.
 __global__ void k_species(const int2* __restrict__ info, int* __restrict__ sidx, int* __restrict__ scount,
-                          const int* __restrict__ soff, int N) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const int t = info[i].y & 0xFF;
-  sidx[soff[t] + atomicAdd(&scount[t], 1)] = i;
+                          const int* __restrict__ soff, int N, int ntype) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int t = i < N ? (info[i].y & 0xFF) : -1;
+  for (int sp = 0; sp < ntype; ++sp) {
+    const unsigned m = __ballot_sync(0xffffffffu, t == sp);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&scount[sp], __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (t == sp) sidx[soff[sp] + base + __popc(m & ((1u << lane) - 1))] = i;
+  }
 }
 
 __device__ __forceinline__ int owner_of(int j, int N, const int* __restrict__ gowner) { return j < N ? j : gowner[j - N]; }
@@ -645,7 +655,8 @@ static int fit_f32_enqueue(nnpe_ctx* c) {
 int nnp_species_enqueue(nnpe_ctx* c) {
   NnpModel* m = c->nnp;
   NNPE_CUDA(c, cudaMemsetAsync(m->d_scount, 0, sizeof(int) * NNPE_MAX_TYPES, c->stream));
-  k_species<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_info, m->d_sidx, m->d_scount, m->d_soff_dev, c->natom);
+  k_species<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_info, m->d_sidx, m->d_scount, m->d_soff_dev, c->natom,
+                                                          c->ntype);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

@@ -710,62 +710,64 @@ __device__ __forceinline__ void prefetch_image(unsigned char* dst, const unsigne
 }
 
 // 128 atoms of one species per CTA; the four weight images stream through two shared buffers so
-// that each image's copy overlaps the MMA chain and epilogue before it.
-__global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
+// that each image's copy overlaps the MMA chain and epilogue before it. 256 threads: row p = t % 128
+// (TMEM lane), half h = t / 128 takes half of each epilogue's columns.
+__global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
+  __shared__ float sEn[2][128];             // per-half partial energies
   unsigned char* sAct = sm;                 // 128 x 256 (G), later 128 x 128 (g2)
   unsigned char* sH1 = sm + 128 * 256 * 2;  // 128 x 128 (h1, later g1)
   unsigned char* sW0 = sH1 + 128 * 128 * 2; // L1, then B2
   unsigned char* sW1 = sW0 + 128 * 256 * 2; // L2, then B1
-  const int t = threadIdx.x, w = t >> 5;
+  const int t = threadIdx.x, w = t >> 5, p = t & 127, half = t >> 7;
   const int sp = f.tile_sp[blockIdx.x], row0 = f.tile_row[blockIdx.x];
   const int M = f.soff[sp + 1] - f.soff[sp];
-  const bool valid = row0 + t < M;
-  const int atom = valid ? f.sidx[f.soff[sp] + row0 + t] : 0;
+  const bool valid = row0 + p < M;
+  const int atom = valid ? f.sidx[f.soff[sp] + row0 + p] : 0;
   const unsigned char* img = f.fit + f.fit_stride * sp;
   const float* sm_c1 = f.small + kFitSmallStride * sp;
   const float *sm_c2 = sm_c1 + 128, *sm_a3 = sm_c1 + 256, *sm_c3 = sm_c1 + 384;
   if (w == 0) tc::tmem_alloc(&tmem_base, 256);
   if (t == 0) tc::mbar_init(&bar, 1);
-  prefetch_image(sW0, img, (int)kImgL1, t, 128);                    // group: L1
-  prefetch_image(sW1, img + kImgL1, (int)kImgL2, t, 128);           // group: L2
-  // G row -> bf16 A tile (K=256)
-  for (int k = 0; k < 256; k += 8) {
+  prefetch_image(sW0, img, (int)kImgL1, t, 256);                    // group: L1
+  prefetch_image(sW1, img + kImgL1, (int)kImgL2, t, 256);           // group: L2
+  // this half of the G row -> bf16 A tile (K=256)
+  for (int k = 128 * half; k < 128 * half + 128; k += 8) {
     float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (valid) {
       const float4 u = *reinterpret_cast<const float4*>(f.G + (size_t)atom * 256 + k);
       const float4 v = *reinterpret_cast<const float4*>(f.G + (size_t)atom * 256 + k + 4);
       g[0] = u.x; g[1] = u.y; g[2] = u.z; g[3] = u.w; g[4] = v.x; g[5] = v.y; g[6] = v.z; g[7] = v.w;
     }
-    *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(t, k, 256)) = tc::pack8(g);
+    *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, k, 256)) = tc::pack8(g);
   }
   tc::cp_async_wait<1>();   // L1 landed
   const uint32_t tmem = tmem_base;
-  const uint32_t taddr = tmem + ((uint32_t)(w * 32) << 16);
+  const uint32_t taddr = tmem + ((uint32_t)((w & 3) * 32) << 16);
   const uint32_t aAct = tc::smem_u32(sAct), aH1 = tc::smem_u32(sH1), aW0 = tc::smem_u32(sW0), aW1 = tc::smem_u32(sW1);
   bool ok = true;
   // L1: z1 = G A1 (+c1), h1 = tanh
   ok = fit_mma(tmem, aAct, 256, aW0, 128, &bar, 0, t, f.ctrl);
-  prefetch_image(sW0, img + kImgL1 + kImgL2, (int)kImgB2, t, 128);   // group: B2 (L1 consumed)
+  prefetch_image(sW0, img + kImgL1 + kImgL2, (int)kImgB2, t, 256);   // group: B2 (L1 consumed)
   if (ok) {
-    for (int c0 = 0; c0 < 128; c0 += 16) {
+    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
       float v[16];
       tc::tmem_ld16(taddr + c0, v);
 #pragma unroll
       for (int q = 0; q < 16; ++q) v[q] = tanh_fast(v[q] + sm_c1[c0 + q]);
-      *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(t, c0, 128)) = tc::pack8(v);
-      *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(t, c0 + 8, 128)) = tc::pack8(v + 8);
+      *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0, 128)) = tc::pack8(v);
+      *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0 + 8, 128)) = tc::pack8(v + 8);
     }
   }
   tc::cp_async_wait<1>();   // L2 landed
   // L2: z2 = h1 A2 (+c2), h2 = tanh, E = h2 A3 + c3, g2 = A3 (1-h2^2)
   if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW1, 128, &bar, 1, t, f.ctrl);
-  prefetch_image(sW1, img + kImgL1 + kImgL2 + kImgB2, (int)kImgB1, t, 128);   // group: B1 (L2 consumed)
+  prefetch_image(sW1, img + kImgL1 + kImgL2 + kImgB2, (int)kImgB1, t, 256);   // group: B1 (L2 consumed)
   if (ok) {
     float e = 0.f;
-    for (int c0 = 0; c0 < 128; c0 += 16) {
+    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
       float v[16];
       tc::tmem_ld16(taddr + 128 + c0, v);
 #pragma unroll
@@ -774,21 +776,22 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
         e += h2 * sm_a3[c0 + q];
         v[q] = sm_a3[c0 + q] * (1.f - h2 * h2);
       }
-      *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(t, c0, 128)) = tc::pack8(v);
-      *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(t, c0 + 8, 128)) = tc::pack8(v + 8);
+      *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, c0, 128)) = tc::pack8(v);
+      *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, c0 + 8, 128)) = tc::pack8(v + 8);
     }
-    if (valid) f.enet[atom] = (double)e + (double)sm_c3[0];
+    sEn[half][p] = e;
   }
   tc::cp_async_wait<1>();   // B2 landed
   // B2: u = g2 A2^T, g1 = u (1-h1^2)
   if (ok) ok = fit_mma(tmem, aAct, 128, aW0, 128, &bar, 0, t, f.ctrl);
+  if (ok && half == 0 && valid) f.enet[atom] = (double)(sEn[0][p] + sEn[1][p]) + (double)sm_c3[0];
   if (ok) {
-    for (int c0 = 0; c0 < 128; c0 += 16) {
+    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
       float v[16];
       tc::tmem_ld16(taddr + c0, v);
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
-        uint4* pchunk = reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(t, c0 + 8 * hh, 128));
+        uint4* pchunk = reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0 + 8 * hh, 128));
         const uint4 hv = *pchunk;
         const __nv_bfloat162* hb = reinterpret_cast<const __nv_bfloat162*>(&hv);
         float gg[8];
@@ -806,7 +809,7 @@ __global__ void __launch_bounds__(128) k_tc_fit(FitTcArgs f) {
   // B1: dE/dG = g1 A1^T (N = 256)
   if (ok) ok = fit_mma(tmem, aH1, 128, aW1, 256, &bar, 1, t, f.ctrl);
   if (ok) {
-    for (int c0 = 0; c0 < 256; c0 += 16) {
+    for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += 16) {
       float v[16];
       tc::tmem_ld16(taddr + c0, v);   // warp-collective: every lane loads, valid rows store
       if (valid) {
@@ -930,7 +933,7 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row; f.G = m->d_G;
   f.fit = t->d_fit; f.fit_stride = t->fit_stride; f.small = t->d_fit_small; f.dG = m->d_dG; f.enet = m->d_enet;
   f.ctrl = c->d_ctrl;
-  k_tc_fit<<<t->ntiles, 128, smem_fit, c->stream>>>(f);
+  k_tc_fit<<<t->ntiles, 256, smem_fit, c->stream>>>(f);
   NNPE_CUDA(c, cudaMemsetAsync(t->d_facc, 0, sizeof(unsigned long long) * 4 * c->natom, c->stream));
   ForceArgs fa;
   fa.pos = c->d_pos; fa.list6 = m->d_list6; fa.n6 = m->d_n6; fa.gowner = c->d_gowner; fa.wdesc = t->d_wdesc64;
