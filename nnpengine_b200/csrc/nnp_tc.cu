@@ -173,7 +173,7 @@ __device__ __forceinline__ bool next_tile(const DescArgs& d, int& a, int& k0, in
 
 // Row p of a tile: its atom, la, list entry and the two positions (loaded ahead of use).
 struct RowFetch {
-  int atom, la;
+  int atom, la, jo;
   bool valid;
   uint32_t ent;
   float4 xi, xj;
@@ -189,10 +189,12 @@ __device__ __forceinline__ void fetch_entry(const DescArgs& d, const TileSeg& s,
     f.xi = __ldg(d.pos + f.atom);
   }
 }
-__device__ __forceinline__ void fetch_xj(const DescArgs& d, RowFetch& f) {
+__device__ __forceinline__ void fetch_xj(const DescArgs& d, RowFetch& f, bool owner = false) {
+  f.jo = 0;
   if (f.valid) {
     const int j = f.ent & NNPE_J_MASK;
     f.xj = __ldg(d.pos + (j < d.npos ? j : 0));
+    if (owner) f.jo = j < d.N ? j : __ldg(d.gowner + (j - d.N < d.npos - d.N ? j - d.N : 0));
   }
 }
 
@@ -466,8 +468,7 @@ __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const 
   r.dcff = 2.f * cf / (den * den);
   r.s = f.ent >> 30;
   r.tj = (f.ent >> 27) & 7;
-  const int j = f.ent & NNPE_J_MASK;
-  r.jo = j < a.N ? j : __ldg(a.gowner + (j - a.N));
+  r.jo = f.jo;
   const float r_rc = 1.f / a.rc, u = r.r * r_rc;
   const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
   const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
@@ -491,14 +492,18 @@ __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const 
   return r;
 }
 
-// dE/dG of the tile's atoms (1 or 2) into sdG[2][256].
-__device__ __forceinline__ void load_tile_dG(const ForceArgs& a, const TileSeg& sg, bool have, float* sdG, int t) {
-  if (!have) return;
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const int k = t + 256 * e, la = k >> 8;
-    if (la == 0 || sg.nb > 0) sdG[k] = __ldg(a.dG + (size_t)(sg.a + la) * 256 + (k & 255));
-  }
+// dE/dG of the tile's atoms (1 or 2): two values per thread, loaded a tile ahead into registers and
+// stored into sdG[2][256] when the tile is built.
+__device__ __forceinline__ float2 fetch_tile_dG(const ForceArgs& a, const TileSeg& sg, bool have, int t) {
+  float2 v = make_float2(0.f, 0.f);
+  if (!have) return v;
+  v.x = __ldg(a.dG + (size_t)sg.a * 256 + t);   // k = t: atom 0, column t (t < 256)
+  if (sg.nb > 0) v.y = __ldg(a.dG + (size_t)(sg.a + 1) * 256 + t);
+  return v;
+}
+__device__ __forceinline__ void store_tile_dG(float2 v, float* sdG, int t) {
+  sdG[t] = v.x;
+  sdG[256 + t] = v.y;
 }
 
 __device__ __forceinline__ float seg_sum(float v) {
@@ -543,12 +548,14 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   RowFetch f0, f1, f2;
   bool have0 = next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg0, t, 256);
   fetch_entry(dv, seg0, have0, p, f0);
-  fetch_xj(dv, f0);
+  fetch_xj(dv, f0, true);
+  const float2 g0 = fetch_tile_dG(a, seg0, have0, t);
   bool have1 = have0 && next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg1, t, 256);
   fetch_entry(dv, seg1, have1, p, f1);
+  float2 g1 = fetch_tile_dG(a, seg1, have1, t);
   ForceRow row0 = force_first_layer(a, f0, sE, sAH, sAH + kTile * kK64 * 2, p, half);
-  load_tile_dG(a, seg0, have0, sdG, t);
-  fetch_xj(dv, f1);
+  if (have0) store_tile_dG(g0, sdG, t);
+  fetch_xj(dv, f1, true);
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
@@ -567,12 +574,14 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     // (1) first layer and dE/dG of tile it+1; loads of tile it+2
     bool have2 = false;
     seg2 = TileSeg{0, 0, 0, 0};
+    float2 g2 = make_float2(0.f, 0.f);
     if (have1) {
       row1 = force_first_layer(a, f1, sE, AH1, AH1 + kTile * kK64 * 2, p, half);
-      load_tile_dG(a, seg1, true, sdG + 512 * b1, t);
+      store_tile_dG(g1, sdG + 512 * b1, t);
       have2 = next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg2, t, 256);
     }
     fetch_entry(dv, seg2, have2, p, f2);
+    g2 = fetch_tile_dG(a, seg2, have2, t);
     // (2) barrier: MMA of tile it complete, stage it+1 written
     tc::fence_async_smem();
     tc::fence_before();
@@ -623,7 +632,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
       if (row0.valid) part = a.scale * (row0.dcff * sy + row0.cff * sk);
     }
     sAcc[half * kTile + p] = part;
-    fetch_xj(dv, f2);
+    fetch_xj(dv, f2, true);
     __syncthreads();
     // (5) half 0: pair forces to j's owner, per-segment sums for the atoms of the tile
     if (half == 0) {
@@ -652,7 +661,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
       }
     }
     seg0 = seg1; have0 = have1; row0 = row1;
-    seg1 = seg2; have1 = have2; f1 = f2;
+    seg1 = seg2; have1 = have2; f1 = f2; g1 = g2;
   }
   tc::fence_before();
   __syncthreads();
