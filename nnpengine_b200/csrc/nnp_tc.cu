@@ -38,7 +38,7 @@ struct NnpTc {
   int* d_tile_row = nullptr;
   int ntiles = 0;
   int* d_soff = nullptr;
-  int ctas_desc = 3, ctas_force = 2;   // CTAs per SM in the grid (shared and tensor memory bound)
+  int ctas_desc = 4, ctas_force = 2;   // CTAs per SM in the grid (shared and tensor memory bound)
   unsigned char* d_wdesc64 = nullptr;  // B image N=64 x K=64: W2_t[q][c] at k=t*32+q (b2 added in the epilogue)
 };
 
@@ -110,20 +110,22 @@ __device__ __forceinline__ void fix_add(unsigned long long* dst, float v) {
 // G is stored once, when its last segment is reduced, so no two CTAs or tiles write it.
 //
 // Per tile t the CTA's 128 threads (row p = thread p) run, in order:
-//   (1) first layer of tile t+1 into operand buffer A[(t+1) % 3]; loads of tile t+2 issued,
-//   (2) barrier, after which MMA 1 of tile t and MMA 2 of tile t-1 are complete,
-//   (3) warp 0: G of tile t-1 out of TMEM[(t-1) % 2], then MMA 1 of tile t+1 into that buffer
-//       (Z = H W2s, K = 64 block-diagonal over the neighbour species; b2 is added in the epilogue),
-//   (4) epilogue of tile t: y = scale cff tanh(z + b2) -> Y (BF16, MN-major) over A[t % 3], and the
+//   (0) wait for MMA 2 of tile t-1 (its operand buffer and TMEM buffer become free),
+//   (1) warp 0: G of tile t-1 out of TMEM[(t-1) % 2]; all: first layer of tile t+1 into operand
+//       buffer A[(t+1) % 2], loads of tile t+2 issued,
+//   (2) barrier, after which MMA 1 of tile t is complete,
+//   (3) MMA 1 of tile t+1 into TMEM[(t+1) % 2] (Z = H W2s, K = 64 block-diagonal over the neighbour
+//       species; b2 is added in the epilogue),
+//   (4) epilogue of tile t: y = scale cff tanh(z + b2) -> Y (BF16, MN-major) over A[t % 2], and the
 //       one-hot S of the (la, s) rows,
 //   (5) barrier; MMA 2 of tile t: TMEM[t % 2] = S Y.
-// MMA 1 of tile t+1 and MMA 2 of tile t run while the threads compute, so the wait of (2) finds
-// them done; three operand buffers and two TMEM buffers keep every buffer out of reach of the MMA
-// that reads it. The activations are BF16 operands of the next MMA, so their tanh is evaluated on
+// MMA 1 of tile t+1 runs during the epilogue of tile t and MMA 2 of tile t during the next
+// iteration's wait; two operand and two TMEM buffers keep every buffer out of reach of the MMA that
+// reads it, and four CTAs per SM overlap each other's waits. The activations are BF16 operands of the next MMA, so their tanh is evaluated on
 // BF16 pairs (one transcendental-unit operation per two values).
 constexpr int kK64 = 64;
 constexpr int kEmbStride4 = 132;   // 16-byte aligned rows of the per-species constants
-constexpr int kDescStages = 3;
+constexpr int kDescStages = 2;
 constexpr int kSmemDesc2 = 64 * kK64 * 2 + kDescStages * kTile * kK64 * 2 + 8 * kTile * 2 + 2 * kEmbStride4 * 4 + 256 * 4;
 
 struct DescArgs {
@@ -264,7 +266,7 @@ __device__ __forceinline__ void desc_readout(const DescArgs& d, uint32_t taddr, 
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(128, 3) k_tc_desc2(DescArgs d) {
+__global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar_z[2], bar_g;
   __shared__ uint32_t tmem_base;
@@ -324,9 +326,16 @@ __global__ void __launch_bounds__(128, 3) k_tc_desc2(DescArgs d) {
   DescRow row1 = row0;
   for (int it = 0; have0 && alive; ++it) {
     const int b0 = it & 1, b1 = b0 ^ 1;
-    unsigned char* A0 = sA + (size_t)(it % 3) * kTile * kK64 * 2;
-    unsigned char* A1 = sA + (size_t)((it + 1) % 3) * kTile * kK64 * 2;
-    // (1) first layer of tile it+1; loads of tile it+2
+    unsigned char* A0 = sA + (size_t)b0 * kTile * kK64 * 2;
+    unsigned char* A1 = sA + (size_t)b1 * kTile * kK64 * 2;
+    // (0) MMA 2 of tile it-1 complete: A[b1] (its Y) free, its G ready in TMEM[b1]
+    if (havep) {
+      alive = cta_wait_mma(&bar_g, ph_g, d.ctrl);
+      ph_g ^= 1;
+      if (!alive) break;
+    }
+    // (1) warp 0: G of tile it-1; all: first layer of tile it+1 into A[b1], loads of tile it+2
+    if (havep && w == 0) desc_readout(d, tmem + 64 * b1, segp, sCarry, lane);
     bool have2 = false;
     seg2 = TileSeg{0, 0, 0, 0};
     if (have1) {
@@ -334,31 +343,26 @@ __global__ void __launch_bounds__(128, 3) k_tc_desc2(DescArgs d) {
       have2 = next_tile(d, ca, ck0, i1, seg2, t);
     }
     fetch_entry(d, seg2, have2, p, f2);
-    // (2) one barrier: A[it+1] written; MMA 1 of tile it and MMA 2 of tile it-1 complete
+    // (2) barrier: A[b1] written, TMEM[b1] read out, MMA 1 of tile it complete
     tc::fence_async_smem();
     tc::fence_before();
     {
       bool ok = true;
       if (t == 0) {
-        ok = tc::mbar_wait(&bar_z[b0], ph_z[b0]) && (!havep || tc::mbar_wait(&bar_g, ph_g));
+        ok = tc::mbar_wait(&bar_z[b0], ph_z[b0]);
         if (!ok) atomicOr(d.ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
       }
       alive = __syncthreads_and(ok) != 0;
     }
     tc::fence_after();
     ph_z[b0] ^= 1;
-    if (havep) ph_g ^= 1;
     if (!alive) break;
-    // (3) warp 0: G of tile it-1 out of TMEM[b1], then MMA 1 of tile it+1 into it
-    if (w == 0) {
-      if (havep) desc_readout(d, tmem + 64 * b1, segp, sCarry, lane);
-      if (have1 && lane == 0) {
-        tc::fence_after();
-        const uint32_t id = tc::idesc_bf16(128, 64);
-        const uint32_t aA = tc::smem_u32(A1);
-        for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem + 64 * b1, tc::tile_desc(aA, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
-        tc::mma_commit(&bar_z[b1]);
-      }
+    // (3) MMA 1 of tile it+1 into TMEM[b1]
+    if (have1 && t == 0) {
+      const uint32_t id = tc::idesc_bf16(128, 64);
+      const uint32_t aA = tc::smem_u32(A1);
+      for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem + 64 * b1, tc::tile_desc(aA, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+      tc::mma_commit(&bar_z[b1]);
     }
     // (4) epilogue of tile it: y = scale cff tanh(z + b2), on BF16 pairs (Y is a BF16 operand)
     const int nrows = seg0.na + seg0.nb, NK = (nrows + 15) & ~15;
