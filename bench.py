@@ -238,10 +238,28 @@ def serve_bench(args, wl):
         th = threading.Thread(target=submitter)
         th.start()
         th.join()
-        srv.drain(3600)
+        t_wait = time.perf_counter()
+        while True:   # progress on stderr while the stream drains
+            try:
+                srv.drain(10.0)
+                break
+            except Exception:
+                inf = srv.info()
+                sys.stderr.write(f"serving: {time.perf_counter() - t_wait:.0f}s after the last arrival: {inf}\n")
+                sys.stderr.flush()
+                if time.perf_counter() - t_wait > args.serve_timeout:
+                    raise RuntimeError(f"served stream not drained after {args.serve_timeout} s: {inf}")
     t_end = time.perf_counter()
     # the server clock (t_submit/t_done) and the host clock differ by a constant offset per request
     stats = [srv.stats(i) for i in ids]
+    first_error = None
+    for i, st in sorted(zip(ids, stats), key=lambda x: x[1]["t_done"]):
+        if st["status"] < 0:
+            try:
+                srv.wait(i, 0.0)
+            except Exception as ex:
+                first_error = f"{ex} (request {i}, {st['natom']} atoms, {st['nsteps']} steps)"
+            break
     lat = np.array([st["t_done"] - st["t_submit"] for st in stats])
     ok = sum(1 for st in stats if st["status"] == 2)
     first_submit = min(st["t_submit"] for st in stats)
@@ -253,7 +271,7 @@ def serve_bench(args, wl):
     return dict(replica_steps_per_s=steps / makespan, atom_steps_per_s=atom_steps / makespan, makespan_s=makespan,
                 p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)), mean_s=float(lat.mean()),
                 completed=ok, requests=nreq, total_steps=steps, total_atom_steps=atom_steps,
-                peak_resident=info["peak_resident"], peak_bytes=info["peak_bytes"], hbm_budget=budget,
+                peak_resident=info["peak_resident"], peak_bytes=info["peak_bytes"], hbm_budget=budget, first_error=first_error,
                 clocks=clk.summary(), wall_after_last_submit_s=t_end - t_arr[-1])
 
 
@@ -336,6 +354,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-scale", type=float, default=1.0, help="multiply every request's step count")
     ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--serve-timeout", type=float, default=900.0)
     ap.add_argument("--drift-ps", type=float, default=0.0, help="after the timed steps, NVE for this many ps")
     ap.add_argument("--target-steps", type=int, default=500)
     ap.add_argument("--rmdf-strength", type=float, default=0.02)
@@ -513,19 +532,20 @@ def main():
         xs = [(x0 + np.float32(k * 0.5) * v0).ravel() for k in range(e2e_steps + 3)]
         for k in range(3):
             x_host.numpy()[:] = xs[k]
-            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), C.byref(erg), None))
+            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), None, None))
         torch.cuda.synchronize()
         h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         h0.record(stream)
-        for k in range(e2e_steps):
+        for k in range(e2e_steps):   # forces every step; the energy only on log steps, as run.cpp:309-342
             x_host.numpy()[:] = xs[3 + k]
-            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), C.byref(erg), None))
+            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), None, None))
         h1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = h0.elapsed_time(h1) / e2e_steps
         e2e = {"value": s.natom * world / (e2e_ms / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": n3 * 4,
-               "d2h_bytes_per_step": n3 * 4 + 8, "ms_per_step": e2e_ms,
-               "call": "nnpe_force_step (positions in, forces + FP64 energy out, list check/rebuild on device)"}
+               "d2h_bytes_per_step": n3 * 4, "ms_per_step": e2e_ms,
+               "call": "nnpe_force_step (positions in, forces out, list check/rebuild on device; energies are "
+                       "evaluated on log steps only, as the reference's step)"}
 
     if rank == 0:
         cpu = None

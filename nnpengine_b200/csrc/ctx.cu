@@ -77,6 +77,7 @@ int nnpe_create(int device, nnpe_ctx** out) {
   if (dev_malloc(c, (void**)&c->d_ctrl, sizeof(int) * CTRL_WORDS) != cudaSuccess ||
       cudaMallocHost(&c->h_ctrl, sizeof(int) * CTRL_WORDS) != cudaSuccess ||
       dev_malloc(c, (void**)&c->d_red, sizeof(double) * 16) != cudaSuccess ||
+      dev_malloc(c, (void**)&c->d_red_part, sizeof(double) * 4 * 256) != cudaSuccess ||
       cudaMallocHost(&c->h_red, sizeof(double) * 16) != cudaSuccess) {
     delete c;
     return NNPE_ECUDA;
@@ -119,7 +120,7 @@ void nnpe_destroy(nnpe_ctx* c) {
   dfree(&c->d_acoef); dfree(&c->d_dcoef); dfree(&c->d_mol_terms); dfree(&c->d_mol_atoms); dfree(&c->d_molshift);
   dfree(&c->d_mol_rep); dfree(&c->d_special); dfree(&c->d_pairtype); dfree(&c->d_emol); dfree(&c->d_wmol);
   dfree(&c->d_gr_counts); dfree(&c->d_gr_counts_inner); dfree(&c->d_gr); dfree(&c->d_sq); dfree(&c->d_gr_norm);
-  dfree(&c->d_qq); dfree(&c->d_ctrl); dfree(&c->d_red); dfree(&c->d_xstage); dfree(&c->d_fstage);
+  dfree(&c->d_qq); dfree(&c->d_ctrl); dfree(&c->d_red); dfree(&c->d_red_part); dfree(&c->d_xstage); dfree(&c->d_fstage);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->h_red) cudaFreeHost(c->h_red);
   if (c->stream) cudaStreamDestroy(c->stream);

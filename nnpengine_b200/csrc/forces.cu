@@ -356,20 +356,41 @@ __device__ double block_sum(double v, double* sh) {
   return r;
 }
 
-__global__ void __launch_bounds__(1024) k_reduce(const double* eatom, const double* watom, const double* kin,
-                                                 const double* emol, const double* wmol, const double* enet, int N,
-                                                 int nmol, int nnet, bool with_kin, double* red, LogRec* log,
-                                                 int log_cap, int* ctrl, bool write_log) {
-  __shared__ double sh[1024];
-  const int t = threadIdx.x;
+// Deterministic two-pass reduction: kReduceBlocks blocks each sum a fixed contiguous share of the
+// per-atom / per-molecule partials in a fixed order, then one block sums the block partials in
+// block order (the same bits on every run).
+constexpr int kReduceBlocks = 256;
+constexpr int kReduceThreads = 256;
+
+__global__ void __launch_bounds__(kReduceThreads) k_reduce_part(const double* eatom, const double* watom, const double* kin,
+                                                                 const double* emol, const double* wmol, const double* enet,
+                                                                 int N, int nmol, int nnet, bool with_kin, double* part) {
+  __shared__ double sh[kReduceThreads];
+  const int t = threadIdx.x, b = blockIdx.x, B = gridDim.x;
   double e = 0, w = 0, k = 0, en = 0;
-  for (int i = t; i < N; i += blockDim.x) { e += eatom[i]; w += watom[i]; if (with_kin) k += kin[i]; }
-  for (int m = t; m < nmol; m += blockDim.x) { e += emol[m]; w += wmol[m]; }
-  for (int m = t; m < nnet; m += blockDim.x) en += enet[m];
+  {
+    const int a0 = (int)((long long)N * b / B), a1 = (int)((long long)N * (b + 1) / B);
+    for (int i = a0 + t; i < a1; i += kReduceThreads) { e += eatom[i]; w += watom[i]; if (with_kin) k += kin[i]; }
+    const int m0 = (int)((long long)nmol * b / B), m1 = (int)((long long)nmol * (b + 1) / B);
+    for (int m = m0 + t; m < m1; m += kReduceThreads) { e += emol[m]; w += wmol[m]; }
+    const int n0 = (int)((long long)nnet * b / B), n1 = (int)((long long)nnet * (b + 1) / B);
+    for (int m = n0 + t; m < n1; m += kReduceThreads) en += enet[m];
+  }
   e = block_sum(e, sh);
   w = block_sum(w, sh);
   k = block_sum(k, sh);
   en = block_sum(en, sh);
+  if (t == 0) {
+    part[4 * b] = e; part[4 * b + 1] = w; part[4 * b + 2] = k; part[4 * b + 3] = en;
+  }
+}
+
+__global__ void __launch_bounds__(kReduceBlocks) k_reduce_final(const double* part, bool with_kin, double* red, LogRec* log,
+                                                                int log_cap, int* ctrl, bool write_log) {
+  __shared__ double sh[kReduceBlocks];
+  const int t = threadIdx.x;
+  const double e = block_sum(part[4 * t], sh), w = block_sum(part[4 * t + 1], sh);
+  const double k = block_sum(part[4 * t + 2], sh), en = block_sum(part[4 * t + 3], sh);
   if (t == 0) {
     red[0] = e + en; red[1] = w; red[3] = en;
     if (with_kin) red[2] = k;
@@ -468,9 +489,12 @@ int energy_reduce_enqueue(nnpe_ctx* c, int mode) {
   const double* enet = c->nnp ? nnp_atom_energy_ptr(c) : nullptr;
   const int nnet = enet ? c->natom : 0;
   const bool bonded = c->d_mol_terms && (c->nbond + c->nangle + c->ndih) > 0;
-  k_reduce<<<1, 1024, 0, c->stream>>>(c->d_eatom, c->d_watom, c->d_kin, c->d_emol, c->d_wmol, enet, c->natom,
-                                      bonded || mode >= 0 ? c->nmol : 0, nnet, mode == 1 || mode == 2, c->d_red,
-                                      c->d_log, c->log_cap, c->d_ctrl, mode == 1 || mode == 3);
+  const bool with_kin = mode == 1 || mode == 2;
+  k_reduce_part<<<kReduceBlocks, kReduceThreads, 0, c->stream>>>(c->d_eatom, c->d_watom, c->d_kin, c->d_emol, c->d_wmol,
+                                                                  enet, c->natom, bonded || mode >= 0 ? c->nmol : 0, nnet,
+                                                                  with_kin, c->d_red_part);
+  k_reduce_final<<<1, kReduceBlocks, 0, c->stream>>>(c->d_red_part, with_kin, c->d_red, c->d_log, c->log_cap, c->d_ctrl,
+                                                     mode == 1 || mode == 3);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

@@ -126,6 +126,7 @@ struct nnpe_ctx {
   double *d_eatom = nullptr, *d_watom = nullptr, *d_kin = nullptr;   // per atom
   double *d_emol = nullptr, *d_wmol = nullptr;                         // per molecule
   double* d_red = nullptr;       // reduction outputs [8]
+  double* d_red_part = nullptr;  // per-block partial sums of the energy reduction [256][4]
   LogRec* d_log = nullptr;
   int log_cap = 0;
   int* d_ctrl = nullptr;

@@ -757,6 +757,13 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
     *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, k, 256)) = tc::pack8(g);
   }
   tc::cp_async_wait<1>();   // L1 landed
+  // The TMEM address that warp 0's alloc wrote is read only after a barrier: the alloc blocks while
+  // CTAs of other kernels on this SM (other streams) hold the columns, and a thread reading the
+  // slot before it is written would take a stale address.
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
   const uint32_t tmem = tmem_base;
   const uint32_t taddr = tmem + ((uint32_t)((w & 3) * 32) << 16);
   const uint32_t aAct = tc::smem_u32(sAct), aH1 = tc::smem_u32(sH1), aW0 = tc::smem_u32(sW0), aW1 = tc::smem_u32(sW1);

@@ -285,9 +285,29 @@ void worker_main(nnpe_server* s) {
     // retire / continue replicas whose chunk completed
     for (size_t k = 0; k < s->resident.size();) {
       Replica* p = s->resident[k].get();
-      if (p->running && cudaEventQuery(p->done) == cudaSuccess) {
-        progressed = true;
-        if (complete_chunk(s, k)) continue;   // erased: same index holds the next replica
+      if (p->running) {
+        const cudaError_t q = cudaEventQuery(p->done);
+        if (q == cudaSuccess) {
+          progressed = true;
+          if (complete_chunk(s, k)) continue;   // erased: same index holds the next replica
+        } else if (q != cudaErrorNotReady) {
+          // the chunk failed (a CUDA error in this context): fail the request instead of waiting on it
+          Request* r = p->req;
+          {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->status = -NNPE_ECUDA;
+            r->err = std::string("chunk failed: ") + cudaGetErrorString(q);
+            r->t_done = s->now();
+            ++s->ndone;
+            s->bytes_parked += p->bytes;
+            s->cv_done.notify_all();
+          }
+          p->running = false;
+          s->parked.push_back(std::move(s->resident[k]));
+          s->resident.erase(s->resident.begin() + k);
+          progressed = true;
+          continue;
+        }
       }
       ++k;
     }
