@@ -672,6 +672,7 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   if (int rc = nnp_species_enqueue(c)) return rc;
   NnpArgs a = make_args(c);
   if (m->bf16) return nnp_tc_forces_enqueue(c, ev);
+  m->g_bf16 = false;
   if (m->kind == 0) {
     k_gauss_desc<<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
   } else {
@@ -705,6 +706,13 @@ int nnpe_nnp_get(nnpe_ctx* c, float* G, float* dG, double* e_atom) {
   NNPE_CUDA(c, cudaMemcpyAsync(d.data(), m->d_dG, sizeof(float) * d.size(), cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaMemcpyAsync(e.data(), m->d_enet, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (m->g_bf16) {   // BF16 rows in the first half of the buffer: widen (exact) from the top down
+    const uint16_t* h = reinterpret_cast<const uint16_t*>(g.data());
+    for (size_t k = g.size(); k-- > 0;) {
+      const uint32_t u = (uint32_t)h[k] << 16;
+      std::memcpy(&g[k], &u, 4);
+    }
+  }
   for (int i = 0; i < N; ++i) {
     const int a = aid[i];
     if (G) std::memcpy(G + (size_t)a * D, g.data() + (size_t)i * D, sizeof(float) * D);

@@ -12,6 +12,7 @@ struct NnpModel {
   int nbin = 0, e1 = 32, e2 = 64, din = 256, h1 = 128, h2 = 128, ntype = 0, npair = 0;
   int cap6 = 256;
   bool bf16 = false;
+  bool g_bf16 = false;       // d_G holds BF16 rows [N][din] (the tensor-core path's descriptor)
   bool enabled = true;
   float* d_embw = nullptr;   // per species: W1[e1] b1[e1] W2[e1][e2] b2[e2]
   float* d_fitw = nullptr;   // per species: A1[din][h1] c1 A2[h1][h2] c2 A3[h2] c3

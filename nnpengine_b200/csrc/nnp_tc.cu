@@ -10,8 +10,10 @@
 //  k_tc_desc2   first layer h1 = tanh(W1 u + b1) per pair into the A tile, block-diagonal over the
 //               neighbour species, so one MMA chain gives every row the second layer of its own
 //               net; epilogue y = scale cff tanh(z + b2) (BF16 pairs); the sum over pairs into G by
-//               atom segment and special class is a second MMA with a one-hot A (no atomics).
-//  k_tc_fit     128 atoms of one species per tile: G -> h1 -> h2 -> E forward and the hand-written
+//               atom segment and special class is a second MMA with a one-hot A (no atomics); G is
+//               stored as BF16 rows, the fitting kernel's operand type.
+//  k_tc_fit     128 atoms of one species per tile (G rows fetched by cp.async straight into the
+//               K-major A tile): G -> h1 -> h2 -> E forward and the hand-written
 //               backward dE/dG = ((A3 (1-h2^2)) A2^T (1-h1^2)) A1^T as four MMA chains (N = 128, 128,
 //               128, 256); activations stay in shared memory, weights stream through two buffers.
 //  k_tc_force2  second layer and its r-derivative per directed pair (two MMAs), the contraction with
@@ -135,7 +137,7 @@ struct DescArgs {
   const int* gowner;
   const unsigned char* wdesc;   // B of MMA 1: N = 64 channels x K = 64, [W2_0; W2_1]
   const float* emb_small;       // per species W1[32] b1[32] b2[64] (stride 128)
-  float* G;
+  uint32_t* G2;                 // descriptor rows [N][256] BF16, two per word (the fitting kernel's operand)
   int* ctrl;
   int cap6, N, ntype, npos;
   float rc, scale;
@@ -144,11 +146,11 @@ struct DescArgs {
 struct TileSeg { int a, k0, na, nb; };
 
 // Next tile of the CTA's range from cursor (a, k0); atoms without pairs are skipped (and get G = 0
-// here when G is given).
-__device__ __forceinline__ bool next_tile_n6(const int* n6, float* G, int& a, int& k0, int i1, TileSeg& s, int t, int nt) {
+// here when G2 is given).
+__device__ __forceinline__ bool next_tile_n6(const int* n6, uint32_t* G2, int& a, int& k0, int i1, TileSeg& s, int t, int nt) {
   while (a < i1 && __ldg(n6 + a) == 0) {
-    if (G)
-      for (int e = t; e < 256; e += nt) G[(size_t)a * 256 + e] = 0.f;
+    if (G2)
+      for (int e = t; e < 128; e += nt) G2[(size_t)a * 128 + e] = 0u;
     ++a;
     k0 = 0;
   }
@@ -170,7 +172,7 @@ __device__ __forceinline__ bool next_tile_n6(const int* n6, float* G, int& a, in
   return true;
 }
 __device__ __forceinline__ bool next_tile(const DescArgs& d, int& a, int& k0, int i1, TileSeg& s, int t) {
-  return next_tile_n6(d.n6, d.G, a, k0, i1, s, t, 128);
+  return next_tile_n6(d.n6, d.G2, a, k0, i1, s, t, 128);
 }
 
 // Row p of a tile: its atom, la, list entry and the two positions (loaded ahead of use).
@@ -254,10 +256,10 @@ __device__ __forceinline__ void desc_readout(const DescArgs& d, uint32_t taddr, 
   }
   __syncwarp();
   if (mine) {
-    if (done) {
-      float4* dst = reinterpret_cast<float4*>(d.G + (size_t)atom * 256 + sc * 64);
+    if (done) {   // BF16 (round to nearest), the rounding the fitting kernel's operand takes
+      uint4* dst = reinterpret_cast<uint4*>(d.G2 + (size_t)atom * 128 + sc * 32);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) dst[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
+      for (int q = 0; q < 8; ++q) dst[q] = tc::pack8(g + 8 * q);
     } else {
 #pragma unroll
       for (int c = 0; c < 64; ++c) sCarry[sc * 64 + c] = g[c];
@@ -692,7 +694,7 @@ struct FitTcArgs {
   const int* soff;
   const int* tile_sp;
   const int* tile_row;
-  const float* G;
+  const uint16_t* G16;   // descriptor rows [N][256] BF16
   const unsigned char* fit;
   size_t fit_stride;
   const float* small;
@@ -744,19 +746,15 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   const float *sm_c2 = sm_c1 + 128, *sm_a3 = sm_c1 + 256, *sm_c3 = sm_c1 + 384;
   if (w == 0) tc::tmem_alloc(&tmem_base, 256);
   if (t == 0) tc::mbar_init(&bar, 1);
+  // this half of the BF16 G row -> A tile (K=256), 16-byte core-matrix rows straight from global
+  for (int k = 128 * half; k < 128 * half + 128; k += 8) {
+    if (valid) tc::cp_async16(sAct + tc::kmajor_off(p, k, 256), f.G16 + (size_t)atom * 256 + k);
+    else *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, k, 256)) = make_uint4(0, 0, 0, 0);
+  }
+  tc::cp_async_commit();                                            // group: G
   prefetch_image(sW0, img, (int)kImgL1, t, 256);                    // group: L1
   prefetch_image(sW1, img + kImgL1, (int)kImgL2, t, 256);           // group: L2
-  // this half of the G row -> bf16 A tile (K=256)
-  for (int k = 128 * half; k < 128 * half + 128; k += 8) {
-    float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (valid) {
-      const float4 u = *reinterpret_cast<const float4*>(f.G + (size_t)atom * 256 + k);
-      const float4 v = *reinterpret_cast<const float4*>(f.G + (size_t)atom * 256 + k + 4);
-      g[0] = u.x; g[1] = u.y; g[2] = u.z; g[3] = u.w; g[4] = v.x; g[5] = v.y; g[6] = v.z; g[7] = v.w;
-    }
-    *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, k, 256)) = tc::pack8(g);
-  }
-  tc::cp_async_wait<1>();   // L1 landed
+  tc::cp_async_wait<1>();   // G and L1 landed
   // The TMEM address that warp 0's alloc wrote is read only after a barrier: the alloc blocks while
   // CTAs of other kernels on this SM (other streams) hold the columns, and a thread reading the
   // slot before it is written would take a stale address.
@@ -946,11 +944,13 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 2 * 256 * 128 * 2;
   DescArgs dd;
   dd.pos = c->d_pos; dd.list6 = m->d_list6; dd.n6 = m->d_n6; dd.gowner = c->d_gowner;
-  dd.wdesc = t->d_wdesc64; dd.emb_small = t->d_emb_small; dd.G = m->d_G; dd.ctrl = c->d_ctrl;
+  dd.wdesc = t->d_wdesc64; dd.emb_small = t->d_emb_small; dd.G2 = reinterpret_cast<uint32_t*>(m->d_G); dd.ctrl = c->d_ctrl;
   dd.cap6 = m->cap6; dd.N = c->natom; dd.ntype = c->ntype; dd.npos = c->natom + c->Gcap; dd.rc = m->rc; dd.scale = m->scale;
   k_tc_desc2<<<std::max(1, std::min(c->natom, sms * t->ctas_desc)), 128, kSmemDesc2, c->stream>>>(dd);
+  m->g_bf16 = true;
   FitTcArgs f;
-  f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row; f.G = m->d_G;
+  f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row;
+  f.G16 = reinterpret_cast<const uint16_t*>(m->d_G);
   f.fit = t->d_fit; f.fit_stride = t->fit_stride; f.small = t->d_fit_small; f.dG = m->d_dG; f.enet = m->d_enet;
   f.ctrl = c->d_ctrl;
   k_tc_fit<<<t->ntiles, 256, smem_fit, c->stream>>>(f);
