@@ -66,6 +66,22 @@ def nnp_flops_per_step(natom, pairs6):
     return pairs6 * per_pair + natom * per_atom
 
 
+def max_over_ranks(x: float, dist=None, device="cuda") -> float:
+    """The largest of the ranks' values (the slowest replica's time): every rank calls it at the
+    same point; without a process group it returns x."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Velocity seed of rank's replica: independent systems of the same workload on each GPU."""
+    return base + 7919 * rank
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -129,13 +145,13 @@ class ClockSampler:
 MIX_SIGMA, MIX_EPS = (3.0, 3.4), (0.15, 0.25)
 
 
-def build_system(wl):
+def build_system(wl, rank=0):
     import cases
     from nnpengine_b200 import systems as S
     if wl.get("mixture"):
-        s = S.lj_mixture(wl["natom"], wl["rho"], 0.6, seed=4)
+        s = S.lj_mixture(wl["natom"], wl["rho"], 0.6, seed=replica_seed(4, rank))
         return s, S.lj_table(2, MIX_SIGMA, MIX_EPS, 10.0, 1000)
-    s = S.water_box(wl["n_side"], wl["bl"], seed=2, nmol=wl.get("nmol"))
+    s = S.water_box(wl["n_side"], wl["bl"], seed=replica_seed(2, rank), nmol=wl.get("nmol"))
     r, F, U = S.water_lj_table(10.0, 1000)
     return s, (r, F, U)
 
@@ -411,7 +427,7 @@ def main():
         dist = dist_mod
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
 
-    s, table = build_system(wl)
+    s, table = build_system(wl, rank)
     e = make_engine(s, table, local, wl.get("nnp"))
     e.pair_exact(args.exact)
     stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
@@ -421,7 +437,7 @@ def main():
     # untimed equilibration of the classical model from the lattice start (Andersen at 300 K,
     # dt 1 fs, the 5 ps of the workload's definition), then the network on and NVE at dt=0.5 fs
     e.verlet(1.0, True)
-    e.thermostat("andersen", 300.0, 300.0, interval=1, frac=0.1, seed=11, total_steps=0)
+    e.thermostat("andersen", 300.0, 300.0, interval=1, frac=0.1, seed=replica_seed(11, rank), total_steps=0)
     if wl.get("nnp"):
         e.nnp_enable(False)
     if args.equil:
@@ -449,11 +465,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1)
-    if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(t0.elapsed_time(t1), dist)
     info = e.list_info()
     nbuild_timed = (log[-1]["nbuild"] if log else info["nbuild"]) - nbuild0
     value = s.natom * args.steps * world / (ms / 1e3)
@@ -477,7 +489,7 @@ def main():
         e.run(nfp, log_interval=nfp, graph=True)
         b.record(stream)
         torch.cuda.synchronize()
-        plain = s.natom * world / (a.elapsed_time(b) / nfp / 1e3)
+        plain = s.natom * world / (max_over_ranks(a.elapsed_time(b), dist) / nfp / 1e3)
         e.nnp_precision(True)
 
     # per-kernel-class device time (CUDA events on the library stream); these launches change the
@@ -541,7 +553,7 @@ def main():
             e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), None, None))
         h1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = h0.elapsed_time(h1) / e2e_steps
+        e2e_ms = max_over_ranks(h0.elapsed_time(h1), dist) / e2e_steps
         e2e = {"value": s.natom * world / (e2e_ms / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": n3 * 4,
                "d2h_bytes_per_step": n3 * 4, "ms_per_step": e2e_ms,
                "call": "nnpe_force_step (positions in, forces out, list check/rebuild on device; energies are "
