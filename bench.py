@@ -104,7 +104,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except FileNotFoundError:
@@ -357,7 +357,7 @@ def time_enqueue(e, stream, which, reps):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="water96k-nnp-bf16", choices=sorted(WORKLOADS))
@@ -484,7 +484,7 @@ def main():
         e.run(5, log_interval=5, graph=True)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        nfp = max(20, args.steps // 4)
+        nfp = min(60, max(20, args.steps // 4))
         a.record(stream)
         e.run(nfp, log_interval=nfp, graph=True)
         b.record(stream)
@@ -546,6 +546,7 @@ def main():
             x_host.numpy()[:] = xs[k]
             e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), None, None))
         torch.cuda.synchronize()
+        nb_e2e0 = e.list_info()["nbuild"]
         h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         h0.record(stream)
         for k in range(e2e_steps):   # forces every step; the energy only on log steps, as run.cpp:309-342
@@ -555,7 +556,8 @@ def main():
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(h0.elapsed_time(h1), dist) / e2e_steps
         e2e = {"value": s.natom * world / (e2e_ms / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": n3 * 4,
-               "d2h_bytes_per_step": n3 * 4, "ms_per_step": e2e_ms,
+               "d2h_bytes_per_step": n3 * 4, "ms_per_step": e2e_ms, "steps": e2e_steps,
+               "list_builds": e.list_info()["nbuild"] - nb_e2e0,
                "call": "nnpe_force_step (positions in, forces out, list check/rebuild on device; energies are "
                        "evaluated on log steps only, as the reference's step)"}
 

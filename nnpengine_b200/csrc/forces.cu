@@ -505,13 +505,26 @@ int check_valid_enqueue(nnpe_ctx* c);
 namespace {
 // positions in atom-id order (host layout) -> sorted master/FP32 coordinates
 __global__ void k_scatter_positions(const float* __restrict__ x, const int* __restrict__ aid, double4* __restrict__ xd,
-                                    float4* __restrict__ pos, int N) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+                                    float4* __restrict__ pos, int N, double bl, bool fp64) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   const int a = aid[k];
   const float px = x[3 * a], py = x[3 * a + 1], pz = x[3 * a + 2];
-  xd[k] = make_double4(px, py, pz, 0);
-  pos[k] = make_float4(px, py, pz, pos[k].w);
+  // the periodic image of the host's position nearest the stored one: the rebuild folds the stored
+  // coordinates into the box and the host's own coordinates need not follow (or may be folded at
+  // other times), so positions stay continuous between list builds
+  const double4 o = xd[k];
+  const double rbl = 1.0 / bl;
+  const double sx = rint((o.x - (double)px) * rbl) * bl, sy = rint((o.y - (double)py) * rbl) * bl,
+               sz = rint((o.z - (double)pz) * rbl) * bl;
+  double4 n;   // no shift (the usual case) stores the host's coordinates unchanged
+  if (fp64) {
+    n = make_double4((double)px + sx, (double)py + sy, (double)pz + sz, 0);
+  } else {   // FP32 state: the float arithmetic of the fold, x - m*bl
+    n = make_double4(__fadd_rn(px, (float)sx), __fadd_rn(py, (float)sy), __fadd_rn(pz, (float)sz), 0);
+  }
+  xd[k] = n;
+  pos[k] = make_float4((float)n.x, (float)n.y, (float)n.z, pos[k].w);
 }
 // sorted forces -> atom-id order
 __global__ void k_gather_forces(const float4* __restrict__ frc, const int* __restrict__ aid, float* __restrict__ f, int N) {
@@ -543,7 +556,7 @@ extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, 
     c->force_step_init = true;
   }
   NNPE_CUDA(c, cudaMemcpyAsync(c->d_xstage, x_host, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, c->stream));
-  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_xstage, c->d_atom_id, c->d_xd, c->d_pos, N);
+  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_xstage, c->d_atom_id, c->d_xd, c->d_pos, N, (double)c->grid.bl, c->fp64_state);
   if (int rc = check_valid_enqueue(c)) return rc;
   if (int rc = rebuild_enqueue(c, true)) return rc;
   if (int rc = ghost_update_enqueue(c, true)) return rc;
