@@ -232,7 +232,8 @@ def serve_bench(args, wl):
     budget = int(min(0.8 * free, 120e9))
     srv = Server(0, ntype=2, table=(F, U), bcoef=[E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)],
                  acoef=[E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)], nnp=NM.embed_model(), bf16=True,
-                 chunk_steps=20, dt=0.5, max_replicas=args.serve_slots, hbm_budget=budget)
+                 chunk_steps=20, dt=0.5, max_replicas=args.serve_slots, hbm_budget=budget,
+                 autotune=not args.no_autotune)
     # warm-up requests (module loading, first graph captures), untimed
     warm = [srv.submit(S.water_request_box(n, 1.0, 90 + k, 300.0), 40, 300.0, k)
             for k, n in enumerate([300, 3000, 30000][:max(1, args.warmup)])]
@@ -365,6 +366,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the plain FP32 network alongside")
     ap.add_argument("--exact", action="store_true", help="pair forces in the reference's exact float sequence")
+    ap.add_argument("--no-autotune", action="store_true", help="default grids for the tensor-core kernels")
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--equil", type=int, default=5000)
     ap.add_argument("--serve-requests", type=int, default=256)
@@ -414,7 +416,7 @@ def main():
             "steps": res["total_steps"], "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded request stream)",
             "config": {"workload": args.workload, "description": wl["desc"], "serve_scale": args.serve_scale,
-                       "slots": args.serve_slots, "timing": "host clock: first arrival to last completion"},
+                       "slots": args.serve_slots, "autotune": not args.no_autotune, "timing": "host clock: first arrival to last completion"},
             "latency_s": {"p50": res["p50_s"], "p99": res["p99_s"], "mean": res["mean_s"]},
             "serving": res, "cpu_baseline": cpu, "clocks": res["clocks"],
             "e2e": {"value": res["replica_steps_per_s"], "unit": "replica-steps/s",
@@ -449,6 +451,9 @@ def main():
     else:
         e.thermostat("none")
         e.verlet(0.5, True)
+    grids = None
+    if wl.get("nnp") == "bf16":
+        grids = e.nnp_autotune(reps=5) if not args.no_autotune else e.nnp_get_grids()
     wlog = e.run(args.warmup, log_interval=max(args.warmup, 1), graph=True)
     nbuild0 = wlog[-1]["nbuild"] if wlog else 0
 
@@ -575,6 +580,8 @@ def main():
                "l2": "inputs larger than L2 (neighbour list %.0f MB)" % (info["entries"] * 4 / 1e6),
                "ns_per_day": value / world / s.natom * 0.5 * 86400 * 1e-6, "kernel_ms": kms,
                "pair_math": "exact float sequence" if args.exact else "rsqrt+FMA (same cutoff test)"}
+        if grids is not None:
+            cfg["tc_grids"] = {"desc": grids[0], "force": grids[1], "autotuned": not args.no_autotune}
         if plain is not None:
             cfg["plain_fp32_value"] = plain
             cfg["bf16_over_fp32"] = value / plain

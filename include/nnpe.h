@@ -216,6 +216,17 @@ int nnpe_nnp_info(nnpe_ctx* ctx, int* din, int* kind);
 /* Pairs inside the network cutoff in the last evaluation (sum over atoms of the full list's count). */
 int64_t nnpe_nnp_pairs(nnpe_ctx* ctx);
 
+/* Grid sizes (CTAs) of the two tensor-core pair kernels (descriptor, force). The reference has no
+ * counterpart: its network runs in TF on one thread. nnpe_nnp_autotune times candidate grids over
+ * `reps` network evaluations of the current state (building the list if it is stale) and keeps the
+ * fastest; with use_cache the choice is shared by contexts of the same device, species count and
+ * half-octave of the atom count within the process. nnpe_nnp_grids sets them (0 = default: 4 and 2
+ * CTAs per SM). The grid fixes how each CTA's pairs are cut into tiles: two runs with the same grid
+ * give the same bits, different grids agree to FP32 rounding of the descriptor sums. */
+int nnpe_nnp_autotune(nnpe_ctx* ctx, int reps, int use_cache, int* grid_desc, int* grid_force);
+int nnpe_nnp_grids(nnpe_ctx* ctx, int grid_desc, int grid_force);
+int nnpe_nnp_get_grids(nnpe_ctx* ctx, int* grid_desc, int* grid_force);
+
 /* Self-test of the tcgen05 tile path on `device`: D[128][N] = bf16(A[128][K]) x bf16(B[N][K])^T,
  * FP32 accumulation in tensor memory (16 <= N <= 256, 16 <= K <= 128, multiples of 16).
  * mode 0: both operands K-major; 1: B MN-major; 2: A rows repeat with period 8 (one 8-row group
@@ -305,6 +316,7 @@ typedef struct nnpe_serve_config {
   int e1, e2, h1, h2;
   const float *coef_p, *coef_w, *coef_d, *coef_r, *embw, *fitw;
   int nnp_bf16;
+  int autotune;              /* tune the network kernels' grids per size class at admission (cached) */
 } nnpe_serve_config;
 
 /* One MD request: a system in the arrays of nnpe_set_system, initial velocities, bonded terms in

@@ -81,6 +81,9 @@ _SIGS = {
     "nnpe_nnp_get": (C.c_int, [_vp, _vp, _vp, _vp]),
     "nnpe_nnp_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "nnpe_nnp_pairs": (C.c_int64, [_vp]),
+    "nnpe_nnp_autotune": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "nnpe_nnp_grids": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "nnpe_nnp_get_grids": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "nnpe_bonded_autogen": (C.c_int, [_vp, C.c_int, _f32p, C.c_int, _f32p, C.c_int, _f32p]),
     "nnpe_profile_enqueue": (C.c_int, [_vp, C.c_int]),
     "nnpe_tc_selftest": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p]),

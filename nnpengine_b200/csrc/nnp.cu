@@ -722,6 +722,31 @@ int nnpe_nnp_get(nnpe_ctx* c, float* G, float* dG, double* e_atom) {
   return NNPE_OK;
 }
 
+int nnpe_sync_errors(nnpe_ctx* c);
+
+// Grid autotuning of the tensor-core kernels on the context's current state (the list is built
+// first when it is stale, and one force evaluation fills the network's pair and species lists).
+// The force array is left holding partial sums: the next force evaluation rewrites it.
+int nnpe_nnp_autotune(nnpe_ctx* c, int reps, int use_cache, int* grid_desc, int* grid_force) {
+  if (!c || !c->have_setup || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_autotune: no network set up");
+  cudaSetDevice(c->device);
+  if (int rc = rebuild_enqueue(c, true)) return rc;
+  if (int rc = ghost_update_enqueue(c, true)) return rc;
+  if (int rc = forces_enqueue(c, false)) return rc;
+  if (int rc = nnpe_sync_errors(c)) return rc;
+  return nnp_tc_autotune(c, reps, use_cache != 0, grid_desc, grid_force);
+}
+
+int nnpe_nnp_grids(nnpe_ctx* c, int grid_desc, int grid_force) {
+  if (!c) return NNPE_EARG;
+  return nnp_tc_set_grids(c, grid_desc, grid_force);
+}
+
+int nnpe_nnp_get_grids(nnpe_ctx* c, int* grid_desc, int* grid_force) {
+  if (!c) return NNPE_EARG;
+  return nnp_tc_get_grids(c, grid_desc, grid_force);
+}
+
 int nnpe_nnp_info(nnpe_ctx* c, int* din, int* kind) {
   if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_info: no network");
   if (din) *din = c->nnp->din;

@@ -52,3 +52,6 @@ struct NnpArgs {
 int nnp_tc_setup(nnpe_ctx* c);
 void nnp_tc_free(NnpModel* m);
 int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev);
+int nnp_tc_autotune(nnpe_ctx* c, int reps, bool use_cache, int* grid_desc, int* grid_force);
+int nnp_tc_set_grids(nnpe_ctx* c, int grid_desc, int grid_force);
+int nnp_tc_get_grids(nnpe_ctx* c, int* grid_desc, int* grid_force);

@@ -22,7 +22,12 @@
 //
 // Every wait on an MMA-completion mbarrier is bounded; on time-out the kernel records
 // NNPE_DEV_TIMEOUT, stops issuing work, frees its tensor memory and returns.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "nnp.cuh"
@@ -41,6 +46,7 @@ struct NnpTc {
   int ntiles = 0;
   int* d_soff = nullptr;
   int ctas_desc = 4, ctas_force = 2;   // CTAs per SM in the grid (shared and tensor memory bound)
+  int grid_desc = 0, grid_force = 0;   // grid sizes chosen by the autotuner or the caller (0: default)
   unsigned char* d_wdesc64 = nullptr;  // B image N=64 x K=64: W2_t[q][c] at k=t*32+q (b2 added in the epilogue)
 };
 
@@ -946,7 +952,8 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   dd.pos = c->d_pos; dd.list6 = m->d_list6; dd.n6 = m->d_n6; dd.gowner = c->d_gowner;
   dd.wdesc = t->d_wdesc64; dd.emb_small = t->d_emb_small; dd.G2 = reinterpret_cast<uint32_t*>(m->d_G); dd.ctrl = c->d_ctrl;
   dd.cap6 = m->cap6; dd.N = c->natom; dd.ntype = c->ntype; dd.npos = c->natom + c->Gcap; dd.rc = m->rc; dd.scale = m->scale;
-  k_tc_desc2<<<std::max(1, std::min(c->natom, sms * t->ctas_desc)), 128, kSmemDesc2, c->stream>>>(dd);
+  const int gdesc = t->grid_desc > 0 ? t->grid_desc : std::max(1, std::min(c->natom, sms * t->ctas_desc));
+  k_tc_desc2<<<gdesc, 128, kSmemDesc2, c->stream>>>(dd);
   m->g_bf16 = true;
   FitTcArgs f;
   f.sidx = m->d_sidx; f.soff = t->d_soff; f.tile_sp = t->d_tile_sp; f.tile_row = t->d_tile_row;
@@ -959,7 +966,7 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   fa.pos = c->d_pos; fa.list6 = m->d_list6; fa.n6 = m->d_n6; fa.gowner = c->d_gowner; fa.wdesc = t->d_wdesc64;
   fa.emb_small = t->d_emb_small; fa.dG = m->d_dG; fa.facc = t->d_facc; fa.ctrl = c->d_ctrl;
   fa.cap6 = m->cap6; fa.N = c->natom; fa.ntype = c->ntype; fa.npos = c->natom + c->Gcap; fa.rc = m->rc; fa.scale = m->scale;
-  const int gforce = std::max(1, std::min(c->natom, sms * t->ctas_force));
+  const int gforce = t->grid_force > 0 ? t->grid_force : std::max(1, std::min(c->natom, sms * t->ctas_force));
   const int gapply = (c->natom + 255) / 256;
   if (ev) {
     k_tc_force2<true><<<gforce, 256, kSmemForce2, c->stream>>>(fa);
@@ -970,6 +977,121 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   }
   NNPE_CHECK_LAUNCH(c);
   return 0;
+}
+
+// Grid autotuner of the two pair kernels. The packed tiles follow each CTA's atom range, so the
+// grid size sets both the load balance and the number of partially filled tiles; the best size
+// depends on the atom count, the pair density and what else shares the device. Candidates: 1-4
+// CTAs per SM for the descriptor kernel (its occupancy limit), 1-2 for the force kernel, and
+// fractions of one wave for small systems; each is timed over `reps` network evaluations of the
+// context's current list with CUDA events, the descriptor grid first with the force grid at its
+// default, then the force grid. A result is cached per (device, species, half-octave of the atom
+// count) for the process, so that replicas of a similar size reuse it. The choice fixes how a
+// CTA's pairs are cut into tiles, so results with different grids agree to FP32 rounding of the
+// descriptor sums, and two runs with the same grid are bit-identical.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tune_cache;
+
+std::vector<int> grid_candidates(int natom, int sms, int max_per_sm) {
+  std::vector<int> v;
+  for (int k = max_per_sm; k >= 1; --k) v.push_back(sms * k);
+  v.push_back(sms / 2);
+  v.push_back(sms / 4);
+  for (int& g : v) g = std::max(1, std::min(natom, g));
+  std::vector<int> u;
+  for (int g : v)
+    if (std::find(u.begin(), u.end(), g) == u.end()) u.push_back(g);
+  return u;
+}
+}  // namespace
+
+int nnpe_sync_errors(nnpe_ctx* c);
+
+int nnp_tc_autotune(nnpe_ctx* c, int reps, bool use_cache, int* grid_desc, int* grid_force) {
+  NnpModel* m = c->nnp;
+  NnpTc* t = m ? m->tc : nullptr;
+  if (!t || !m->bf16) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_autotune: the BF16 tensor-core network is not active");
+  const int sms = nnpe_sm_count(c->device);
+  const auto key = std::make_tuple(c->device, c->ntype, (int)std::floor(2.0 * std::log2((double)std::max(c->natom, 1))));
+  if (use_cache) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      t->grid_desc = std::min(it->second.first, c->natom);
+      t->grid_force = std::min(it->second.second, c->natom);
+      c->graph_valid = false;
+      if (grid_desc) *grid_desc = t->grid_desc;
+      if (grid_force) *grid_force = t->grid_force;
+      return NNPE_OK;
+    }
+  }
+  reps = std::max(1, reps);
+  cudaEvent_t a, b;
+  NNPE_CUDA(c, cudaEventCreate(&a));
+  NNPE_CUDA(c, cudaEventCreate(&b));
+  auto time_now = [&](float* ms) -> int {
+    if (int rc = nnp_tc_forces_enqueue(c, false)) return rc;   // warm
+    NNPE_CUDA(c, cudaEventRecord(a, c->stream));
+    for (int r = 0; r < reps; ++r)
+      if (int rc = nnp_tc_forces_enqueue(c, false)) return rc;
+    NNPE_CUDA(c, cudaEventRecord(b, c->stream));
+    NNPE_CUDA(c, cudaEventSynchronize(b));
+    NNPE_CUDA(c, cudaEventElapsedTime(ms, a, b));
+    return 0;
+  };
+  int rc = 0;
+  int best_d = 0, best_f = 0;
+  float best = 1e30f, ms = 0.f;
+  t->grid_force = 0;
+  for (int g : grid_candidates(c->natom, sms, t->ctas_desc)) {
+    t->grid_desc = g;
+    if ((rc = time_now(&ms))) break;
+    if (ms < best) { best = ms; best_d = g; }
+  }
+  if (!rc) {
+    t->grid_desc = best_d;
+    best = 1e30f;
+    for (int g : grid_candidates(c->natom, sms, t->ctas_force)) {
+      t->grid_force = g;
+      if ((rc = time_now(&ms))) break;
+      if (ms < best) { best = ms; best_f = g; }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) {
+    t->grid_desc = t->grid_force = 0;
+    return rc;
+  }
+  t->grid_force = best_f;
+  c->graph_valid = false;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = {best_d, best_f};
+  }
+  if (grid_desc) *grid_desc = best_d;
+  if (grid_force) *grid_force = best_f;
+  return nnpe_sync_errors(c);
+}
+
+int nnp_tc_set_grids(nnpe_ctx* c, int grid_desc, int grid_force) {
+  NnpTc* t = c->nnp ? c->nnp->tc : nullptr;
+  if (!t) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_grids: no tensor-core network");
+  if (grid_desc < 0 || grid_force < 0) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_grids: negative grid");
+  t->grid_desc = grid_desc > 0 ? std::min(grid_desc, std::max(c->natom, 1)) : 0;
+  t->grid_force = grid_force > 0 ? std::min(grid_force, std::max(c->natom, 1)) : 0;
+  c->graph_valid = false;
+  return NNPE_OK;
+}
+
+int nnp_tc_get_grids(nnpe_ctx* c, int* grid_desc, int* grid_force) {
+  NnpTc* t = c->nnp ? c->nnp->tc : nullptr;
+  if (!t) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_grids: no tensor-core network");
+  const int sms = nnpe_sm_count(c->device);
+  if (grid_desc) *grid_desc = t->grid_desc > 0 ? t->grid_desc : std::max(1, std::min(c->natom, sms * t->ctas_desc));
+  if (grid_force) *grid_force = t->grid_force > 0 ? t->grid_force : std::max(1, std::min(c->natom, sms * t->ctas_force));
+  return NNPE_OK;
 }
 
 namespace {

@@ -137,6 +137,10 @@ int setup_replica(nnpe_server* s, Request* r, nnpe_ctx** out) {
       return rc;
     if ((rc = nnpe_nnp_precision(ctx, c.nnp_bf16))) return rc;
   }
+  if (c.autotune && c.nnp_kind >= 0 && c.nnp_bf16) {
+    // before the first chunk is captured; a size class tuned once serves later replicas from the cache
+    if ((rc = nnpe_nnp_autotune(ctx, 3, 1, nullptr, nullptr))) return rc;
+  }
   if ((rc = nnpe_verlet_setup(ctx, c.dt, c.fp64_state))) return rc;
   if ((rc = nnpe_thermostat(ctx, c.thermostat, r->temperature, r->temperature, c.thermostat ? c.chunk_steps : 0,
                             c.thermo_frac, r->seed)))

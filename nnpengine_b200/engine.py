@@ -157,6 +157,20 @@ class Engine:
     def nnp_precision(self, bf16: bool):
         self._ok(self.lib.nnpe_nnp_precision(self.h, int(bf16)))
 
+    def nnp_autotune(self, reps: int = 5, use_cache: bool = True):
+        """Tune the tensor-core kernels' grid sizes on the current state; returns (desc, force) CTAs."""
+        gd, gf = C.c_int(0), C.c_int(0)
+        self._ok(self.lib.nnpe_nnp_autotune(self.h, reps, int(use_cache), C.byref(gd), C.byref(gf)))
+        return gd.value, gf.value
+
+    def nnp_grids(self, grid_desc: int = 0, grid_force: int = 0):
+        self._ok(self.lib.nnpe_nnp_grids(self.h, grid_desc, grid_force))
+
+    def nnp_get_grids(self):
+        gd, gf = C.c_int(0), C.c_int(0)
+        self._ok(self.lib.nnpe_nnp_get_grids(self.h, C.byref(gd), C.byref(gf)))
+        return gd.value, gf.value
+
     def nnp_get(self):
         din, kind = C.c_int(0), C.c_int(0)
         self._ok(self.lib.nnpe_nnp_info(self.h, C.byref(din), C.byref(kind)))

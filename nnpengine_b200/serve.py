@@ -26,7 +26,7 @@ class ServeConfig(C.Structure):
                 ("natyp", C.c_int), ("acoef", _fp), ("ndtyp", C.c_int), ("dcoef", _fp), ("nnp_kind", C.c_int),
                 ("nnp_cutoff", C.c_double), ("nnp_nbin", C.c_int), ("nnp_scale", C.c_double), ("e1", C.c_int),
                 ("e2", C.c_int), ("h1", C.c_int), ("h2", C.c_int), ("coef_p", _fp), ("coef_w", _fp), ("coef_d", _fp),
-                ("coef_r", _fp), ("embw", _fp), ("fitw", _fp), ("nnp_bf16", C.c_int)]
+                ("coef_r", _fp), ("embw", _fp), ("fitw", _fp), ("nnp_bf16", C.c_int), ("autotune", C.c_int)]
 
 
 class Request(C.Structure):
@@ -75,7 +75,8 @@ class Server:
                  bcoef: Sequence = (), acoef: Sequence = (), dcoef: Sequence = (), nnp=None, nnp_cutoff: float = 6.0,
                  nnp_nbin: int = 750, bf16: bool = True, pair_cutoff: float = 10.0, skin: float = 2.0,
                  neigh_cap: int = 1024, dt: float = 0.5, fp64: bool = True, thermostat: bool = True,
-                 thermo_frac: float = 0.1, max_replicas: int = 64, hbm_budget: int = 64 << 30, chunk_steps: int = 20):
+                 thermo_frac: float = 0.1, max_replicas: int = 64, hbm_budget: int = 64 << 30, chunk_steps: int = 20,
+                 autotune: bool = False):
         self.lib = _lib.load()
         for name, (res, args) in _SIGS.items():
             fn = getattr(self.lib, name)
@@ -86,6 +87,7 @@ class Server:
         cfg.device, cfg.max_replicas, cfg.hbm_budget, cfg.chunk_steps = device, max_replicas, int(hbm_budget), chunk_steps
         cfg.pair_cutoff, cfg.skin, cfg.neigh_cap, cfg.dt = pair_cutoff, skin, neigh_cap, dt
         cfg.fp64_state, cfg.thermostat, cfg.thermo_frac, cfg.ntype = int(fp64), int(thermostat), thermo_frac, ntype
+        cfg.autotune = int(autotune)
         if table is not None:
             F, U = (np.ascontiguousarray(a, np.float32) for a in table)
             cfg.nbin, cfg.force, cfg.potential = F.shape[1] - 1, self._f(F), self._f(U)

@@ -181,3 +181,34 @@ def test_embed_nnp_bf16_sparse_and_dense_pair_counts(rho):
     e.compute_forces(True)   # deterministic
     G2, _, _ = e.nnp_get()
     np.testing.assert_array_equal(G, G2)
+
+
+def test_autotuned_grids_same_bits_for_same_grid_and_bf16_bar_across_grids():
+    """The grid autotuner picks grid sizes among its candidates; a second context given the same grids
+    reproduces the forces bit for bit, and the default grids agree to well inside the BF16 bar."""
+    s, _ = cases.water_case(jitter=0.05)
+    m = NM.embed_model()
+    tuned = nnp_engine(s, model=m)
+    tuned.nnp_precision(True)
+    gd, gf = tuned.nnp_autotune(reps=2, use_cache=False)
+    sms = 148
+    assert 1 <= gd <= min(s.natom, 4 * sms) and 1 <= gf <= min(s.natom, 2 * sms)
+    assert tuned.nnp_get_grids() == (gd, gf)
+    tuned.compute_forces(True)
+    f_tuned = tuned.forces().copy()
+    fixed = nnp_engine(s, model=m)
+    fixed.nnp_precision(True)
+    fixed.nnp_grids(gd, gf)
+    fixed.list_build()
+    fixed.compute_forces(True)
+    np.testing.assert_array_equal(fixed.forces(), f_tuned)
+    default = nnp_engine(s, model=m)
+    default.nnp_precision(True)
+    default.list_build()
+    default.compute_forces(True)
+    assert default.nnp_get_grids() == (min(s.natom, 4 * sms), min(s.natom, 2 * sms))
+    assert cases.rel_rms(default.forces(), f_tuned) < 2e-3
+    r, _, _, _ = _bf16_vs_fp64(s, m, fixed)
+    assert cases.rel_rms(f_tuned, r["f"]) < 1e-2
+    for e in (tuned, fixed, default):
+        assert e.device_errors() == 0

@@ -125,3 +125,16 @@ def test_arrivals_join_while_others_run():
         assert st["t_admit"] < lst["t_done"] and st["t_done"] < lst["t_done"]
     assert srv.info()["peak_resident"] >= 2
     srv.close()
+
+
+def test_autotuned_server_completes_and_reuses_the_tuning():
+    syss = systems()
+    srv = server(max_replicas=4, autotune=True)
+    ids = [srv.submit(s, n, t, seed) for s, (_, _, t, n, seed) in zip(syss, REQS)]
+    again = srv.submit(syss[0], REQS[0][3], REQS[0][2], REQS[0][4])   # same size class: cached grids
+    srv.drain(600)
+    for s, i in zip(syss + [syss[0]], ids + [again]):
+        x, v, st = srv.result(i, s.natom)
+        assert st["status"] == 2
+        assert np.all(np.isfinite(x)) and np.all(np.isfinite(v))
+    srv.close()
