@@ -202,7 +202,8 @@ def read_ref_dump(d: str) -> Dict[str, np.ndarray]:
                      ("sq.f32", np.float32), ("qq.f32", np.float32), ("rr.f32", np.float32), ("log_e.f64", np.float64),
                      ("log_w.f64", np.float64), ("log_k.f64", np.float64), ("log_enn.f64", np.float64),
                      ("log_exp.f64", np.float64), ("rmdf_erg.f64", np.float64), ("rmdf_sq.f32", np.float32),
-                     ("tbl_force.f32", np.float32), ("tbl_pot.f32", np.float32)]:
+                     ("tbl_force.f32", np.float32), ("tbl_pot.f32", np.float32), ("sqd_q.f32", np.float32),
+                     ("sqd_sq.f32", np.float32), ("sqd_count.i32", np.int32)]:
         p = os.path.join(d, name)
         if os.path.exists(p):
             out[name.split(".")[0]] = np.fromfile(p, dt)
@@ -263,3 +264,60 @@ def rmdf_tables(st, fq, Fbase, Ubase, potential=True):
     if potential:
         U[:, :nbin] += fq @ st["potmx"].T
     return F, U
+
+
+# ----------------------------------------------------------------------------------------------
+# SQD (direct S(q) over reciprocal lattice vectors, grsq.cpp:362-585) restated in FP64
+# ----------------------------------------------------------------------------------------------
+
+def sqd_gvectors(bl, nq, qmax):
+    """The reference's G set and bins (grsq.cpp:362-470): half-space integer triples (k>0; k=0,j>0;
+    k=j=0,i>0) with i^2+j^2+k^2 <= (int)(qmax/g)^2, g = 2 pi/L, the cutoff, |G| and the bin edges in
+    its float arithmetic. Returns (ijk int[ngv][3], |G| float32[ngv], bin int[ngv])."""
+    f = np.float32
+    g = f(f(2 * np.pi) / f(bl))
+    ratio = f(f(qmax) / g)
+    kc = int(ratio)
+    cut = int(f(ratio * ratio))
+    r = np.arange(-kc, kc + 1)
+    I, J, K = np.meshgrid(r, r, r, indexing="ij")
+    I, J, K = I.ravel(), J.ravel(), K.ravel()
+    n2 = I * I + J * J + K * K
+    half = (K > 0) | ((K == 0) & (J > 0)) | ((K == 0) & (J == 0) & (I > 0))
+    sel = half & (n2 <= cut)
+    ijk = np.stack([I[sel], J[sel], K[sel]], 1)
+    gscl = (np.sqrt(n2[sel].astype(np.float32)) * g).astype(np.float32)
+    dq = f(f(qmax) / f(nq))
+    edges = (np.arange(nq, dtype=np.float32) * dq).astype(np.float32)   # i*dq in float, i = 0..nq-1
+    b = np.searchsorted(edges, gscl, side="right") - 1                   # largest i with edge_i <= |G|
+    return ijk, gscl, np.clip(b, 0, nq - 1)
+
+
+def sqd(x, typ, ntype, bl, nq, qmax, chunk=4096):
+    """FP64 restatement of SQD::compute: per G and type, S_t = sum sin(G.x), C_t = sum cos(G.x);
+    per bin and type pair (t1 <= t2), sq = mean over the bin's G of (S1 S2 + C1 C2) * N/(n1 n2)
+    minus N/n1 when t1 == t2. Returns (q = mean |G| per bin, sq [nq][npair], count per bin)."""
+    ijk, gscl, b = sqd_gvectors(bl, nq, qmax)
+    x = np.asarray(x, np.float64)
+    typ = np.asarray(typ)
+    n = np.bincount(typ, minlength=ntype).astype(np.float64)
+    N = float(len(typ))
+    pairs = [(i, j) for i in range(ntype) for j in range(i, ntype)]
+    acc = np.zeros((nq, len(pairs)))
+    G = ijk.astype(np.float64) * (2 * np.pi / float(np.float32(bl)))
+    for s0 in range(0, len(G), chunk):
+        ph = G[s0:s0 + chunk] @ x.T
+        sn, cs = np.sin(ph), np.cos(ph)
+        S = np.stack([sn[:, typ == t].sum(1) for t in range(ntype)], 1)
+        Cc = np.stack([cs[:, typ == t].sum(1) for t in range(ntype)], 1)
+        for p, (i, j) in enumerate(pairs):
+            np.add.at(acc[:, p], b[s0:s0 + chunk], S[:, i] * S[:, j] + Cc[:, i] * Cc[:, j])
+    count = np.bincount(b, minlength=nq)
+    qsum = np.bincount(b, weights=gscl.astype(np.float64), minlength=nq)
+    q = np.where(count > 0, qsum / np.maximum(count, 1), 0.0)
+    sq = np.zeros((nq, len(pairs)))
+    for p, (i, j) in enumerate(pairs):
+        fac = N / (n[i] * n[j])
+        base = N / n[j] if i == j else 0.0
+        sq[:, p] = np.where(count > 0, acc[:, p] / np.maximum(count, 1) * fac - base, 0.0)
+    return q, sq, count

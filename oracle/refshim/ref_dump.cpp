@@ -53,6 +53,8 @@ struct Cfg {
   std::vector<std::string> rmdf_files;
   float rmdf_strength = 0, rmdf_gamma = 1;
   int gr_interval = 0, gr_interval_long = 0;
+  int sqd_nq = 0;          // direct S(q) (SQD, grsq.cpp:362-585) of the final state when > 0
+  float sqd_qmax = 0;
 };
 
 void die(const char* m) { fprintf(stderr, "ref_dump: %s\n", m); exit(2); }
@@ -84,6 +86,7 @@ Cfg parse(const char* path) {
     } else if (k == "gr_interval") {
       if (sscanf(line, "%*s %d %d", &c.gr_interval, &c.gr_interval_long) != 2) die("bad gr_interval line");
     }
+    else if (k == "sqd") { if (sscanf(line, "%*s %d %f", &c.sqd_nq, &c.sqd_qmax) != 2) die("bad sqd line"); }
     else if (k == "cutoff") fl(c.cutoff);
     else if (k == "skin") fl(c.skin);
     else if (k == "gr_cutoff") fl(c.gr_cutoff);
@@ -458,12 +461,25 @@ int main(int argc, char** argv) {
     }
     dump(c, "rmdf_sq.f32", rmdf->sq[0], (size_t)c.rmdf_files.size() * sq.nbin_q);
   }
+  int sqd_ngv = 0;
+  if (c.sqd_nq > 0) {   // as run.cpp:420-432: SQD of the final positions, computed by every thread
+    SQD sqd(c.sqd_nq, c.sqd_qmax);
+#pragma omp parallel num_threads(NT)
+    { sqd.compute(omp_get_thread_num()); }
+    std::vector<int> cnt(sqd.nbin_q);
+    for (int i = 0; i < sqd.nbin_q; ++i) cnt[i] = sqd.vend[i] - sqd.vbegin[i];
+    dump(c, "sqd_q.f32", sqd.qq, (size_t)sqd.nbin_q);
+    dump(c, "sqd_sq.f32", sqd.sq[0], (size_t)sqd.nbin_q * ENVIRON::npair);
+    dump(c, "sqd_count.i32", cnt.data(), cnt.size());
+    sqd.dump((c.out + "/sqd.txt").c_str(), false);
+    sqd_ngv = sqd.ngv;
+  }
   FILE* fp = fopen((c.out + "/info.txt").c_str(), "w");
   fprintf(fp, "natom %d\nnghost %d\nntot %d\nnum_gx %d\nnpair %d\nnbin_r %d\nnbin_r_inner %d\nnbin_q %d\n"
-          "full_pairs %lld\nnbuild_last %d\nt_loop %.9f\nsteps %d\nthreads %d\n",
+          "full_pairs %lld\nnbuild_last %d\nt_loop %.9f\nsteps %d\nthreads %d\nsqd_ngv %d\n",
           ENVIRON::natom, ENVIRON::nghost, ENVIRON::ntot, ENVIRON::num_gx, ENVIRON::npair, gr.nbin_r,
           gr.nbin_r_inner, sq.nbin_q, total_pairs_full, log_build.empty() ? 0 : log_build.back(), t_loop,
-          total_steps, NT);
+          total_steps, NT, sqd_ngv);
   fclose(fp);
   return 0;
 }

@@ -26,7 +26,12 @@ is run on the seeded cases of tests/cases.py; its outputs are stored compactly:
                  RMDF (strength 0.02, gamma 0.5) and the nnp_run mode with the tabulated NNP and RMDF
                  on its pair tables; its log lines and the line counts of its output files.
 
-Run:  python tests/golden/make_golden.py   (needs /root/reference/src and `make -C oracle ref`).
+* sqd648.npz, sqd2000.npz  the reference's direct S(q) (SQD, grsq.cpp:362-585) of the 648-atom water
+                 box (jittered, 60 bins to 6 A^-1) and of the 2000-atom mixture (40 bins to 3 A^-1):
+                 the positions it used, mean |G| per bin, S(q) per type pair and G count per bin.
+
+Run:  python tests/golden/make_golden.py [name ...]   (needs /root/reference/src and
+`make -C oracle ref`; without names every fixture is written).
 """
 from __future__ import annotations
 
@@ -157,10 +162,34 @@ def nnp_gauss648(work):
     print("nnp_gauss648: network energy", float(snap["log_enn"][0]))
 
 
+def _sqd_fixture(work, name, s, table, nq, qmax):
+    f = cases.write_inputs(s, table, work)
+    cfg = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10,
+           "velocity": f["vel"], "mode": "md", "steps": 0, "dt": 0.5, "log_interval": 1, "sqd": f"{nq} {qmax}"}
+    if s.moltypes[0].n_atom > 1:
+        cfg.update(bonded_cfg())
+    r = orc.run_ref_dump(cfg, work)
+    out = dict(x=r["x"].reshape(-1, 3), typ=s.typ, bl=np.float32(s.bl), nq=nq, qmax=np.float32(qmax),
+               q=r["sqd_q"], sq=r["sqd_sq"].reshape(nq, -1), count=r["sqd_count"], ngv=r["info"]["sqd_ngv"])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name + ":", s.natom, "atoms,", out["ngv"], "G vectors")
+
+
+def sqd648(work):
+    s, table = cases.water_case(jitter=0.05)
+    _sqd_fixture(work, "sqd648", s, table, 60, 6.0)
+
+
+def sqd2000(work):
+    s, table = cases.mixture_case()
+    _sqd_fixture(work, "sqd2000", s, table, 40, 3.0)
+
+
+ALL = [water648, mixture2000, nnp_gauss648, rmdf2000, driver648, sqd648, sqd2000]
+
 if __name__ == "__main__":
+    names = sys.argv[1:]
     with tempfile.TemporaryDirectory() as t:
-        water648(os.path.join(t, "w"))
-        mixture2000(os.path.join(t, "m"))
-        nnp_gauss648(os.path.join(t, "n"))
-        rmdf2000(os.path.join(t, "r"))
-        driver648(os.path.join(t, "d"))
+        for fn in ALL:
+            if not names or fn.__name__ in names:
+                fn(os.path.join(t, fn.__name__))

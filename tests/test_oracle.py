@@ -160,3 +160,18 @@ def test_restated_rmdf_matches_reference():
     from nnpengine_b200 import systems as S
     q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, 2, seed=7)
     np.testing.assert_array_equal(sqex, g["sqex"])
+
+
+@pytest.mark.parametrize("name,ntype", [("sqd648", 2), ("sqd2000", 2)])
+def test_restated_sqd_matches_reference(name, ntype):
+    """The FP64 SQD restatement on the positions the reference used reproduces its G set per bin
+    exactly, its mean |G| to float rounding, and its S(q) to the reference's float accumulation."""
+    g = np.load(os.path.join(cases.GOLDEN, name + ".npz"))
+    nq = int(g["nq"])
+    q, sq, cnt = orc.sqd(g["x"], g["typ"], ntype, float(g["bl"]), nq, float(g["qmax"]))
+    np.testing.assert_array_equal(cnt, g["count"])
+    assert int(cnt.sum()) == int(g["ngv"])
+    m = cnt > 0
+    np.testing.assert_allclose(q[m], g["q"][m], rtol=1e-5)
+    scale = max(1.0, float(np.abs(g["sq"]).max()))
+    assert np.abs(sq[m] - g["sq"][m]).max() < 1e-4 * scale
