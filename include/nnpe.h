@@ -252,6 +252,16 @@ int nnpe_gr_nbin(const nnpe_ctx* ctx, int inner);
 int nnpe_gr_get(nnpe_ctx* ctx, int inner, uint64_t* counts, double* gr);
 int nnpe_sq_compute(nnpe_ctx* ctx, int inner, double* sq, double* q);
 
+/* ---- SQD (grsq.h:40-61): S(q) summed directly over reciprocal lattice vectors -------------
+ * nnpe_sqd_setup is the SQD ctor (grsq.cpp:362-489): the half-space G set with |G| <= q_max, binned
+ * on nq points, returns the vector count. nnpe_sqd_compute is SQD::compute (grsq.cpp:542-573) on the
+ * current positions; nnpe_sqd_get returns the mean |G| per bin [nq], S(q) [nq][npair] (FP64) and
+ * the vectors per bin [nq] (empty bins hold 0); nnpe_sqd_dump is SQD::dump (grsq.cpp:575-608). */
+int nnpe_sqd_setup(nnpe_ctx* ctx, int nq, double qmax, int* ngv);
+int nnpe_sqd_compute(nnpe_ctx* ctx);
+int nnpe_sqd_get(nnpe_ctx* ctx, double* q, double* sq, int* count);
+int nnpe_sqd_dump(nnpe_ctx* ctx, const char* fname, int append);
+
 /* ---- RMDF (grsq.h:82-112): reverse-MD / FMIRL refinement of the pair table ---------------
  * RMDF ctor (grsq.cpp:899-1059) from arrays: n_sq targets, per q point (the SQ grid) S_exp, the
  * weight wt (multiplied by strength) and ntype scattering factors ff[n][q][t]. gamma = 1 is DA/RMD,

@@ -81,6 +81,10 @@ _SIGS = {
     "nnpe_nnp_get": (C.c_int, [_vp, _vp, _vp, _vp]),
     "nnpe_nnp_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "nnpe_nnp_pairs": (C.c_int64, [_vp]),
+    "nnpe_sqd_setup": (C.c_int, [_vp, C.c_int, C.c_double, C.POINTER(C.c_int)]),
+    "nnpe_sqd_compute": (C.c_int, [_vp]),
+    "nnpe_sqd_get": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nnpe_sqd_dump": (C.c_int, [_vp, C.c_char_p, C.c_int]),
     "nnpe_nnp_autotune": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "nnpe_nnp_grids": (C.c_int, [_vp, C.c_int, C.c_int]),
     "nnpe_nnp_get_grids": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

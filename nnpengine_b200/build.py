@@ -30,6 +30,7 @@ UNITS = {
     "integrate.cu": EXACT,
     "gr.cu": EXACT,
     "rmdf.cu": EXACT,
+    "sqd.cu": EXACT,
     "serve.cu": [],
     "nnp.cu": [],
     "nnp_tc.cu": [],

@@ -116,6 +116,7 @@ void nnpe_destroy(nnpe_ctx* c) {
   free_state(c);
   nnp_free(c);
   rmdf_free(c);
+  sqd_free(c);
   dfree(&c->d_table); dfree(&c->d_bond); dfree(&c->d_angle); dfree(&c->d_dih); dfree(&c->d_bcoef);
   dfree(&c->d_acoef); dfree(&c->d_dcoef); dfree(&c->d_mol_terms); dfree(&c->d_mol_atoms); dfree(&c->d_molshift);
   dfree(&c->d_mol_rep); dfree(&c->d_special); dfree(&c->d_pairtype); dfree(&c->d_emol); dfree(&c->d_wmol);

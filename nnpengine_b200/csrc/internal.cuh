@@ -54,6 +54,7 @@ struct LogRec {
 
 struct NnpModel;   // network term (nnp.cu)
 struct RmdfState;  // structure-factor refinement (rmdf.cu)
+struct SqdState;   // direct S(q) over reciprocal lattice vectors (sqd.cu)
 
 struct nnpe_ctx {
   int device = 0;
@@ -146,6 +147,7 @@ struct nnpe_ctx {
   NnpModel* nnp = nullptr;
   // RMDF refinement of the pair table (d_red[4] holds the last erg_exp)
   RmdfState* rmdf = nullptr;
+  SqdState* sqd = nullptr;
   // device bytes held by this context (dev_malloc / dev_free)
   int64_t dev_bytes = 0;
   // CUDA graphs of the step variants
@@ -225,3 +227,4 @@ void nnp_free(nnpe_ctx* c);
 cudaError_t dev_malloc(nnpe_ctx* c, void** p, size_t bytes);
 void dev_free(void* p);
 void rmdf_free(nnpe_ctx* c);
+void sqd_free(nnpe_ctx* c);

@@ -13,8 +13,8 @@
 // formats (environ.cpp:178-188, grsq.cpp:221-256, 324-360, 1380-1416, pair.cpp:421-437).
 //
 // Differences: the velocity generator is seeded (--seed; the reference seeds from random_device,
-// main.cpp:16); positions and velocities advance in FP64 unless --fp32-state; the direct S(q)
-// (`sqd`) output line is read but not computed. A non-zero status from the library ends the program
+// main.cpp:16); positions and velocities advance in FP64 unless --fp32-state. A non-zero status
+// from the library ends the program
 // with its message, as END_PROGRAM does (util.cpp:117-124).
 #include <cmath>
 #include <cstdint>
@@ -333,8 +333,19 @@ int main(int argc, char** argv) {
     dump_avg(f1, app, q, sq, npair);
   }
   l = next_line(fp);
-  if (sscanf(l.c_str(), "%s", f1) != 1) die("input", "read error (sqd)");
-  if (f1[0] != '*') fprintf(stderr, "sqd = %s: the direct S(q) is not part of this build; skipped\n", f1);
+  {  // file append q_max nq (run.cpp:420-432)
+    float sqd_qmax = 0;
+    int sqd_nq = 0;
+    if (sscanf(l.c_str(), "%s %d %f %d", f1, &app, &sqd_qmax, &sqd_nq) != 4) die("input", "read error (sqd)");
+    if (f1[0] != '*') {
+      fprintf(stderr, "sqd = %s; append = %d\n", f1, (int)(app != 0));
+      int ngv = 0;
+      ok(nnpe_sqd_setup(g_ctx, sqd_nq, sqd_qmax, &ngv), "SQD::SQD");
+      fprintf(stderr, "SQDIRECT::SQDIRECT %d G vecs\n", ngv);
+      ok(nnpe_sqd_compute(g_ctx), "SQD::compute");
+      ok(nnpe_sqd_dump(g_ctx, f1, app), "SQD::dump");
+    }
+  }
   l = next_line(fp);
   if (sscanf(l.c_str(), "%s %d", f1, &app) != 2) die("input", "read error (sqx)");
   if (f1[0] != '*' && nsq > 0) ok(nnpe_rmdf_dump_sq(g_ctx, f1, app), "RMDF::dumpSQ");

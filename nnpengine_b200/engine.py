@@ -157,6 +157,26 @@ class Engine:
     def nnp_precision(self, bf16: bool):
         self._ok(self.lib.nnpe_nnp_precision(self.h, int(bf16)))
 
+    # ---- SQD (direct S(q)) -------
+    def sqd_setup(self, nq: int, qmax: float) -> int:
+        n = C.c_int(0)
+        self._ok(self.lib.nnpe_sqd_setup(self.h, nq, qmax, C.byref(n)))
+        self._sqd_nq = nq
+        return n.value
+
+    def sqd_compute(self):
+        """S(q) of the current positions: (mean |G| per bin, sq [nq][npair], vectors per bin)."""
+        self._ok(self.lib.nnpe_sqd_compute(self.h))
+        nq, npair = self._sqd_nq, int(self.lib.nnpe_npair(self.h))
+        q = np.zeros(nq)
+        sq = np.zeros(nq * npair)
+        cnt = np.zeros(nq, np.int32)
+        self._ok(self.lib.nnpe_sqd_get(self.h, q.ctypes.data, sq.ctypes.data, cnt.ctypes.data))
+        return q, sq.reshape(nq, npair), cnt
+
+    def sqd_dump(self, path: str, append: bool = False):
+        self._ok(self.lib.nnpe_sqd_dump(self.h, path.encode(), int(append)))
+
     def nnp_autotune(self, reps: int = 5, use_cache: bool = True):
         """Tune the tensor-core kernels' grid sizes on the current state; returns (desc, force) CTAs."""
         gd, gf = C.c_int(0), C.c_int(0)

@@ -103,10 +103,11 @@ def write_nnp_inputs(m, d):
 
 
 def write_run_input(d, mode, s, table=None, nnp_paths=None, temps=(0.0, 0.0), steps=(20, 5, 20, 5, 10),
-                    rmdf=None, nbin=1000, cutoffs=(10.0, 2.0, 10.0), nq=512, qmax=20.0):
+                    rmdf=None, nbin=1000, cutoffs=(10.0, 2.0, 10.0), nq=512, qmax=20.0, sqd=None):
     """The run input file of the reference's `classical` or `nnp_run` mode (run.cpp:25-50) for a
     case in directory d; rmdf = (strength, gamma, target file) or None (no target: n_sq 0, which
-    the reference reads but cannot run, so its harness runs use one target of strength 0)."""
+    the reference reads but cannot run, so its harness runs use one target of strength 0);
+    sqd = (q_max, nq) writes the direct S(q) of the final state, None skips it."""
     os.makedirs(d, exist_ok=True)
     init = os.path.join(d, "init.txt")
     S.write_init_file(init, s)
@@ -124,8 +125,9 @@ def write_run_input(d, mode, s, table=None, nnp_paths=None, temps=(0.0, 0.0), st
         lines += [f"{rmdf[0]} {rmdf[1]}", f"1 {rmdf[2]}", os.path.join(d, "no_such_delta.txt")]
     lines.append(f"{temps[0]} {temps[1]}")
     lines.append(" ".join(str(v) for v in steps))
-    out = {k: os.path.join(d, k + ".out") for k in ("xyz", "gr", "sq", "sqx", "force")}
-    lines += [f"{out['xyz']} 0", f"{out['gr']} 0", f"{out['sq']} 0", "* 0 20 10", f"{out['sqx']} 0"]
+    out = {k: os.path.join(d, k + ".out") for k in ("xyz", "gr", "sq", "sqd", "sqx", "force")}
+    sqd_line = f"{out['sqd']} 0 {sqd[0]} {sqd[1]}" if sqd else "* 0 20 10"   # file append q_max nq
+    lines += [f"{out['xyz']} 0", f"{out['gr']} 0", f"{out['sq']} 0", sqd_line, f"{out['sqx']} 0"]
     if mode == "classical":
         lines.append(f"{out['force']} 0")
     path = os.path.join(d, "run.in")

@@ -189,6 +189,7 @@ def test_autotuned_grids_same_bits_for_same_grid_and_bf16_bar_across_grids():
     s, _ = cases.water_case(jitter=0.05)
     m = NM.embed_model()
     tuned = nnp_engine(s, model=m)
+    tuned.set_bonded(s, [], [], [])   # the network term alone, as the FP64 oracle has it
     tuned.nnp_precision(True)
     gd, gf = tuned.nnp_autotune(reps=2, use_cache=False)
     sms = 148
@@ -197,12 +198,14 @@ def test_autotuned_grids_same_bits_for_same_grid_and_bf16_bar_across_grids():
     tuned.compute_forces(True)
     f_tuned = tuned.forces().copy()
     fixed = nnp_engine(s, model=m)
+    fixed.set_bonded(s, [], [], [])
     fixed.nnp_precision(True)
     fixed.nnp_grids(gd, gf)
     fixed.list_build()
     fixed.compute_forces(True)
     np.testing.assert_array_equal(fixed.forces(), f_tuned)
     default = nnp_engine(s, model=m)
+    default.set_bonded(s, [], [], [])
     default.nnp_precision(True)
     default.list_build()
     default.compute_forces(True)
