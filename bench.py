@@ -49,6 +49,10 @@ WORKLOADS = {
                                "to 15 A in 0.01 A bins (uint64 counts) every step (cell-based every 10), S(q) on 512 "
                                "points in FP64, RMDF (gamma 1) against the weighted S(q) of the same liquid with eps "
                                "x1.1, Andersen 300 K, dt 1 fs"),
+    "sqd96k": dict(sqd=True, n_side=32, bl=99.3, nmol=32000, nnp=None, nq=512, qmax=10.0, cpu_qmax=1.2,
+                   desc="direct S(q) (SQD) of the 96,000-atom water box: every reciprocal lattice vector of the "
+                        "half space with |G| <= 10 A^-1 (2 pi/L spacing), S_t and C_t per type summed over all atoms, "
+                        "512 bins; one step = one evaluation on the current positions"),
     "serve256": dict(serve=True, nnp="bf16",
                      desc="served replica stream: 256 seeded requests, water boxes of log-uniform 300-30,000 atoms at "
                           "0.95-1.05 g/cm^3 and 250-400 K (Andersen every 20 steps), 100-5000 steps each (uniform "
@@ -208,6 +212,58 @@ def cpu_reference(wl, steps: int):
     return (s.natom * n / t, int(out["info"]["threads"]),
             f"{n} MD steps of the {s.natom}-atom system ({what}), MD loop only, {out['info']['threads']} OpenMP "
             f"threads on a {ncpu}-CPU host")
+
+
+def cpu_sqd_reference(wl):
+    """The reference's SQD (grsq.cpp:362-573, its OpenMP code in oracle/_ref) on the same positions, at
+    a smaller q_max so that the sample takes seconds; returns (atom-G evaluations/s, threads, sample)."""
+    from oracle import orc
+    import cases
+    s, table = build_system(wl)
+    with tempfile.TemporaryDirectory() as d:
+        f = cases.write_inputs(s, table, d)
+        cfg = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10,
+               "velocity": f["vel"], "mode": "md", "steps": 0, "dt": 0.5, "log_interval": 1,
+               "sqd": f"{wl['nq']} {wl['cpu_qmax']}"}
+        out = orc.run_ref_dump(cfg, os.path.join(d, "o"), fast=True, timeout=1800)
+    info = out["info"]
+    rate = s.natom * int(info["sqd_ngv"]) / float(info["t_sqd"])
+    return rate, int(info["threads"]), (f"SQD of the {s.natom}-atom box at q_max {wl['cpu_qmax']} A^-1 "
+                                        f"({int(info['sqd_ngv'])} G vectors), {info['threads']} OpenMP threads on a "
+                                        f"{os.cpu_count()}-CPU host")
+
+
+def sqd_bench(args, wl, local):
+    """Direct S(q) on the device: atom-G evaluations per second over K evaluations (CUDA events on the
+    library stream), the same through nnpe_sqd_compute with its result copied back (e2e)."""
+    import torch
+    s, table = build_system(wl)
+    e = make_engine(s, table, local, None)
+    stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
+    ngv = e.sqd_setup(wl["nq"], wl["qmax"])
+    for _ in range(args.warmup):
+        e.lib.nnpe_sqd_compute(e.h)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for _ in range(args.steps):   # each call also copies the per-bin result back and synchronises
+            e._ok(e.lib.nnpe_sqd_compute(e.h))
+        t1.record(stream)
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    evals = s.natom * ngv
+    value = evals / (ms / 1e3)
+    # arithmetic per atom-G pair: one complex multiply (4 mul/fma) + two adds = 8 FLOP; nominal FP32
+    # CUDA-core peak 148 SMs x 128 lanes x 2 x 1.965 GHz
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    ach = evals * 8 / (ms / 1e3) / 1e12
+    e.close()
+    return dict(value=value, ms=ms, ngv=ngv, clocks=clk.summary(),
+                roofline={"bound": "fp32", "kernel": "k_sqd_runs + k_sqd_bins", "achieved": ach, "peak": peak,
+                          "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                          "peak_source": "nominal FP32 CUDA-core rate (no measured FP32 peak on this pool)",
+                          "alg_flops_per_launch": evals * 8})
 
 
 def serve_bench(args, wl):
@@ -387,18 +443,41 @@ def main():
         if rank != 0:
             return
         cwl = (WORKLOADS["water3k-classical"] | {"nnp": "bf16"}) if wl.get("serve") else wl
-        rate, threads, sample = cpu_reference(cwl, args.cpu_steps)
+        unit = "atom-G evaluations/s" if wl.get("sqd") else "atom-steps/s"
+        rate, threads, sample = cpu_sqd_reference(wl) if wl.get("sqd") else cpu_reference(cwl, args.cpu_steps)
         print(json.dumps({
-            "impl": "reference", "metric": "atom-steps/s", "value": rate, "unit": "atom-steps/s", "n_gpus": args.gpus,
+            "impl": "reference", "metric": unit, "value": rate, "unit": unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "description": wl["desc"]},
-            "cpu_baseline": {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference", "sample": sample},
-            "e2e": {"value": rate, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+            "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
     import torch
     torch.cuda.set_device(local)
+    if wl.get("sqd"):
+        if rank != 0:
+            return
+        r = sqd_bench(args, wl, local)
+        cpu = None
+        if not args.no_cpu_baseline:
+            rate, threads, sample = cpu_sqd_reference(wl)
+            cpu = {"value": rate, "unit": "atom-G evaluations/s", "cores": threads, "kind": "reference", "sample": sample}
+        nq = wl["nq"]
+        print(json.dumps({
+            "metric": "atom-G evaluations/s", "value": r["value"], "unit": "atom-G evaluations/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 phases and bin sums)",
+            "data": "synthetic (seeded water box, lattice start)",
+            "config": {"workload": args.workload, "description": wl["desc"], "natom": 96000, "g_vectors": r["ngv"],
+                       "nq": nq, "qmax": wl["qmax"], "l2": "inputs in L2 (1.5 MB of positions); compute-bound"},
+            "roofline": r["roofline"], "cpu_baseline": cpu, "clocks": r["clocks"],
+            "e2e": {"value": r["value"], "unit": "atom-G evaluations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": nq * 3 * 8, "note": "positions are device-resident; each step returns "
+                    "the per-bin S(q) to the host inside the timed region"},
+            "gpu_launches": 2 * args.steps}))
+        return
     if wl.get("serve"):
         if rank != 0:
             return

@@ -12,7 +12,7 @@
 // axis. One thread owns a run. The CTA stages the atoms (FP64 fractional coordinates, type, and
 // the unit phasor e^{2 pi i u} along each axis) in shared memory, and every thread walks them in
 // the same order: per atom one sincospi of the run's first phase, reduced to [-1/2, 1/2) turns in
-// FP64, then 15 complex multiplications by the axis phasor give the run's other vectors. The sums
+// FP64, then one complex multiplication by the axis phasor per further vector. The sums
 // over atoms are FP32 per thread (the reference sums in float too); the products per bin are summed
 // in FP64 by one warp per bin over its vectors in a fixed order, so results are deterministic.
 #include <algorithm>
@@ -99,12 +99,12 @@ __global__ void __launch_bounds__(kSqdThreads) k_sqd_runs(const double4* __restr
         float sn, cs;
         sincospif((float)(2.0 * turns), &sn, &cs);
         const float2 e = ph[axis][j];
+        // every run steps the full length (a shorter run's extra sums are never stored), so the
+        // inner loop carries no predicates: two adds and one complex multiply per vector
 #pragma unroll
         for (int k = 0; k < kRunLen; ++k) {
-          if (k < len) {
-            s[k] += sn;
-            c[k] += cs;
-          }
+          s[k] += sn;
+          c[k] += cs;
           const float c2 = fmaf(cs, e.x, -sn * e.y), s2 = fmaf(sn, e.x, cs * e.y);
           cs = c2;
           sn = s2;

@@ -462,10 +462,13 @@ int main(int argc, char** argv) {
     dump(c, "rmdf_sq.f32", rmdf->sq[0], (size_t)c.rmdf_files.size() * sq.nbin_q);
   }
   int sqd_ngv = 0;
+  double t_sqd = 0;
   if (c.sqd_nq > 0) {   // as run.cpp:420-432: SQD of the final positions, computed by every thread
     SQD sqd(c.sqd_nq, c.sqd_qmax);
+    const auto ts = std::chrono::steady_clock::now();
 #pragma omp parallel num_threads(NT)
     { sqd.compute(omp_get_thread_num()); }
+    t_sqd = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
     std::vector<int> cnt(sqd.nbin_q);
     for (int i = 0; i < sqd.nbin_q; ++i) cnt[i] = sqd.vend[i] - sqd.vbegin[i];
     dump(c, "sqd_q.f32", sqd.qq, (size_t)sqd.nbin_q);
@@ -476,10 +479,10 @@ int main(int argc, char** argv) {
   }
   FILE* fp = fopen((c.out + "/info.txt").c_str(), "w");
   fprintf(fp, "natom %d\nnghost %d\nntot %d\nnum_gx %d\nnpair %d\nnbin_r %d\nnbin_r_inner %d\nnbin_q %d\n"
-          "full_pairs %lld\nnbuild_last %d\nt_loop %.9f\nsteps %d\nthreads %d\nsqd_ngv %d\n",
+          "full_pairs %lld\nnbuild_last %d\nt_loop %.9f\nsteps %d\nthreads %d\nsqd_ngv %d\nt_sqd %.9f\n",
           ENVIRON::natom, ENVIRON::nghost, ENVIRON::ntot, ENVIRON::num_gx, ENVIRON::npair, gr.nbin_r,
           gr.nbin_r_inner, sq.nbin_q, total_pairs_full, log_build.empty() ? 0 : log_build.back(), t_loop,
-          total_steps, NT, sqd_ngv);
+          total_steps, NT, sqd_ngv, t_sqd);
   fclose(fp);
   return 0;
 }
