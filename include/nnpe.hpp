@@ -299,6 +299,21 @@ class SQ {
     if (thread_id == 0) check(nnpe_sq_compute(ENVIRON::ctx, 0, nullptr, nullptr), "SQ::compute", ENVIRON::ctx);
   }
 };
+// SQD (grsq.h:40-61): S(q) summed over reciprocal lattice vectors, of the positions at compute().
+class SQD {
+ public:
+  int nbin_q, ngv = 0;
+  numtype q_max;
+  SQD(int nq, numtype qmax) : nbin_q(nq), q_max(qmax) {
+    check(nnpe_sqd_setup(ENVIRON::ctx, nq, qmax, &ngv), "SQD::SQD", ENVIRON::ctx);
+  }
+  void compute(int thread_id) {
+    if (thread_id == 0) check(nnpe_sqd_compute(ENVIRON::ctx), "SQD::compute", ENVIRON::ctx);
+  }
+  void dump(const char* fname, bool append = false) {
+    check(nnpe_sqd_dump(ENVIRON::ctx, fname, append), "SQD::dump", ENVIRON::ctx);
+  }
+};
 class RMDF {
  public:
   bool on;

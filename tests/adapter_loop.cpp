@@ -1,7 +1,8 @@
 // Test program: the classical step loop of run.cpp:204-394 written against the reference's classes
 // as nnpe.hpp provides them (one thread, NVE, no g(r) steps), for a water box:
-//   adapter_loop <init-file> <table-file> <total_steps> <log_interval> <positions-out>
-// Prints the log lines of run.cpp:383-390 and writes the final positions (float32, atom-id order).
+//   adapter_loop <init-file> <table-file> <total_steps> <log_interval> <positions-out> [sqd-out]
+// Prints the log lines of run.cpp:383-390 and writes the final positions (float32, atom-id order);
+// with sqd-out, the direct S(q) of the final state to 6 A^-1 on 60 points (run.cpp:420-432).
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -11,7 +12,7 @@
 using namespace nnpe;
 
 int main(int argc, char** argv) {
-  if (argc != 6) return 2;
+  if (argc != 6 && argc != 7) return 2;
   const int total_steps = std::atoi(argv[3]), log_interval = std::atoi(argv[4]);
   const numtype pair_cutoff = 10, skin = 2, gr_cutoff = 10;
   ENVIRON::initialize(argv[1]);
@@ -82,6 +83,11 @@ int main(int argc, char** argv) {
   FILE* fp = std::fopen(argv[5], "wb");
   std::fwrite(x.data(), sizeof(float), x.size(), fp);
   std::fclose(fp);
+  if (argc == 7) {
+    SQD sqd(60, 6.0f);
+    sqd.compute(0);
+    sqd.dump(argv[6]);
+  }
   nnpe_destroy(ENVIRON::ctx);
   return 0;
 }

@@ -74,7 +74,9 @@ def test_reference_style_loop_through_adapter_matches_step_loop(tmp_path):
     s, table = cases.water_case()
     f = cases.write_inputs(s, table, str(tmp_path / "in"))
     xout = str(tmp_path / "x.f32")
-    r = subprocess.run([exe, f["init"], f["table"], "20", "5", xout], capture_output=True, text=True, timeout=600)
+    sqd_out = str(tmp_path / "sqd_adapter.txt")
+    r = subprocess.run([exe, f["init"], f["table"], "20", "5", xout, sqd_out], capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     log = cases.parse_log(r.stdout)
     x_adapter = np.fromfile(xout, np.float32).reshape(-1, 3)
@@ -88,4 +90,8 @@ def test_reference_style_loop_through_adapter_matches_step_loop(tmp_path):
     ref = e.run(21, log_interval=5)
     np.testing.assert_array_equal(x_adapter, e.positions())
     np.testing.assert_allclose(log[:, 3], [r["erg"] for r in ref], rtol=1e-6)
+    e.sqd_setup(60, 6.0)   # the adapter's SQD of the same final state: the same file
+    e.sqd_compute()
+    e.sqd_dump(str(tmp_path / "sqd_engine.txt"))
+    assert open(sqd_out).read() == open(str(tmp_path / "sqd_engine.txt")).read()
     e.close()
