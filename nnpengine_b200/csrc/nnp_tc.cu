@@ -709,33 +709,46 @@ struct FitTcArgs {
   int* ctrl;
 };
 
+// One MMA chain of the fitting kernel: thread 0 waits for the weight image's bulk copy (wbar,
+// wphase), issues the chain and waits for its completion; false (and NNPE_DEV_TIMEOUT) when either
+// bounded wait gave up.
 __device__ __forceinline__ bool fit_mma(uint32_t tmem, uint32_t aA, int KA, uint32_t aB, int N, uint64_t* bar, uint32_t phase,
-                                        int t, int* ctrl) {
+                                        uint64_t* wbar, uint32_t wphase, int t, int* ctrl) {
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
+  bool got = true;
   if (t == 0) {
-    const uint32_t id = tc::idesc_bf16(128, N);
-    for (int kk = 0; kk < KA / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(aA, KA, kk), tc::tile_desc(aB, KA, kk), id, kk > 0);
-    tc::mma_commit(bar);
+    got = tc::mbar_wait(wbar, wphase);
+    if (got) {
+      const uint32_t id = tc::idesc_bf16(128, N);
+      for (int kk = 0; kk < KA / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(aA, KA, kk), tc::tile_desc(aB, KA, kk), id, kk > 0);
+      tc::mma_commit(bar);
+      got = tc::mbar_wait(bar, phase);
+    }
+    if (!got) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_TIMEOUT);
   }
-  return cta_wait_mma(bar, phase, ctrl);
+  const bool ok = __syncthreads_and(got) != 0;
+  tc::fence_after();
+  return ok;
 }
 
-
-// Weight image -> shared memory with cp.async (16 B per copy), one commit group per call.
-__device__ __forceinline__ void prefetch_image(unsigned char* dst, const unsigned char* src, int bytes, int t, int nt) {
-  for (int k = t; k < bytes / 16; k += nt) tc::cp_async16(dst + 16 * k, src + 16 * k);
-  tc::cp_async_commit();
+// Weight image -> shared memory: thread 0 arms the buffer's barrier with the image size and issues
+// bulk copies of at most 32 KB (the tensor core is the only reader, so no proxy fence is needed).
+__device__ __forceinline__ void load_image(unsigned char* dst, const unsigned char* src, uint32_t bytes, uint64_t* bar) {
+  tc::mbar_arrive_expect_tx(bar, bytes);
+  for (uint32_t off = 0; off < bytes; off += 32768u)
+    tc::bulk_g2s(dst + off, src + off, min(32768u, bytes - off), bar);
 }
 
-// 128 atoms of one species per CTA; the four weight images stream through two shared buffers so
-// that each image's copy overlaps the MMA chain and epilogue before it. 256 threads: row p = t % 128
-// (TMEM lane), half h = t / 128 takes half of each epilogue's columns.
+// 128 atoms of one species per CTA; the four weight images stream through two shared buffers by
+// bulk copies (one barrier per buffer, two phases each) so that each copy overlaps the MMA chain and
+// epilogue before it. 256 threads: row p = t % 128 (TMEM lane), half h = t / 128 takes half of each
+// epilogue's columns.
 __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   extern __shared__ __align__(128) unsigned char sm[];
-  __shared__ uint64_t bar;
+  __shared__ uint64_t bar, bar_w[2];
   __shared__ uint32_t tmem_base;
   __shared__ float sEn[2][128];             // per-half partial energies
   unsigned char* sAct = sm;                 // 128 x 256 (G), later 128 x 128 (g2)
@@ -749,18 +762,24 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   const int atom = valid ? f.sidx[f.soff[sp] + row0 + p] : 0;
   const unsigned char* img = f.fit + f.fit_stride * sp;
   const float* sm_c1 = f.small + kFitSmallStride * sp;
-  const float *sm_c2 = sm_c1 + 128, *sm_a3 = sm_c1 + 256, *sm_c3 = sm_c1 + 384;
+  const float *sm_c2 = sm_c1 + 128, *sm_c3 = sm_c1 + 384, *sm_a3 = sm_c1 + 256;
+  int issued0 = 0, issued1 = 0;             // bulk loads per buffer (thread 0)
   if (w == 0) tc::tmem_alloc(&tmem_base, 256);
-  if (t == 0) tc::mbar_init(&bar, 1);
+  if (t == 0) {
+    tc::mbar_init(&bar, 1);
+    tc::mbar_init(&bar_w[0], 1);
+    tc::mbar_init(&bar_w[1], 1);
+    load_image(sW0, img, (uint32_t)kImgL1, &bar_w[0]);            // buffer 0, phase 0: L1
+    load_image(sW1, img + kImgL1, (uint32_t)kImgL2, &bar_w[1]);   // buffer 1, phase 0: L2
+    issued0 = issued1 = 1;
+  }
   // this half of the BF16 G row -> A tile (K=256), 16-byte core-matrix rows straight from global
   for (int k = 128 * half; k < 128 * half + 128; k += 8) {
     if (valid) tc::cp_async16(sAct + tc::kmajor_off(p, k, 256), f.G16 + (size_t)atom * 256 + k);
     else *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, k, 256)) = make_uint4(0, 0, 0, 0);
   }
-  tc::cp_async_commit();                                            // group: G
-  prefetch_image(sW0, img, (int)kImgL1, t, 256);                    // group: L1
-  prefetch_image(sW1, img + kImgL1, (int)kImgL2, t, 256);           // group: L2
-  tc::cp_async_wait<1>();   // G and L1 landed
+  tc::cp_async_commit();
+  tc::cp_async_wait<0>();   // G landed
   // The TMEM address that warp 0's alloc wrote is read only after a barrier: the alloc blocks while
   // CTAs of other kernels on this SM (other streams) hold the columns, and a thread reading the
   // slot before it is written would take a stale address.
@@ -773,8 +792,8 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   const uint32_t aAct = tc::smem_u32(sAct), aH1 = tc::smem_u32(sH1), aW0 = tc::smem_u32(sW0), aW1 = tc::smem_u32(sW1);
   bool ok = true;
   // L1: z1 = G A1 (+c1), h1 = tanh
-  ok = fit_mma(tmem, aAct, 256, aW0, 128, &bar, 0, t, f.ctrl);
-  prefetch_image(sW0, img + kImgL1 + kImgL2, (int)kImgB2, t, 256);   // group: B2 (L1 consumed)
+  ok = fit_mma(tmem, aAct, 256, aW0, 128, &bar, 0, &bar_w[0], 0, t, f.ctrl);
+  if (ok && t == 0) { load_image(sW0, img + kImgL1 + kImgL2, (uint32_t)kImgB2, &bar_w[0]); ++issued0; }   // B2
   if (ok) {
     for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
       float v[16];
@@ -785,10 +804,12 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
       *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0 + 8, 128)) = tc::pack8(v + 8);
     }
   }
-  tc::cp_async_wait<1>();   // L2 landed
   // L2: z2 = h1 A2 (+c2), h2 = tanh, E = h2 A3 + c3, g2 = A3 (1-h2^2)
-  if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW1, 128, &bar, 1, t, f.ctrl);
-  prefetch_image(sW1, img + kImgL1 + kImgL2 + kImgB2, (int)kImgB1, t, 256);   // group: B1 (L2 consumed)
+  if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW1, 128, &bar, 1, &bar_w[1], 0, t, f.ctrl);
+  if (ok && t == 0) {   // B1
+    load_image(sW1, img + kImgL1 + kImgL2 + kImgB2, (uint32_t)kImgB1, &bar_w[1]);
+    ++issued1;
+  }
   if (ok) {
     float e = 0.f;
     for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
@@ -805,9 +826,8 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
     }
     sEn[half][p] = e;
   }
-  tc::cp_async_wait<1>();   // B2 landed
   // B2: u = g2 A2^T, g1 = u (1-h1^2)
-  if (ok) ok = fit_mma(tmem, aAct, 128, aW0, 128, &bar, 0, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem, aAct, 128, aW0, 128, &bar, 0, &bar_w[0], 1, t, f.ctrl);
   if (ok && half == 0 && valid) f.enet[atom] = (double)(sEn[0][p] + sEn[1][p]) + (double)sm_c3[0];
   if (ok) {
     for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
@@ -829,9 +849,8 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
       }
     }
   }
-  tc::cp_async_wait<0>();   // B1 landed
   // B1: dE/dG = g1 A1^T (N = 256)
-  if (ok) ok = fit_mma(tmem, aH1, 128, aW1, 256, &bar, 1, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem, aH1, 128, aW1, 256, &bar, 1, &bar_w[1], 1, t, f.ctrl);
   if (ok) {
     for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += 16) {
       float v[16];
@@ -843,7 +862,12 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
       }
     }
   }
-  tc::cp_async_wait<0>();
+  if (!ok && t == 0) {
+    // a wait gave up: let the bulk loads still in flight land (bounded) before the CTA exits. A
+    // buffer's phases complete in order, so waiting for the parity of its last load covers both.
+    if (issued0) tc::mbar_wait(&bar_w[0], (uint32_t)((issued0 - 1) & 1), 200000000ll);
+    if (issued1) tc::mbar_wait(&bar_w[1], (uint32_t)((issued1 - 1) & 1), 200000000ll);
+  }
   tc::fence_before();
   __syncthreads();
   if (w == 0) tc::tmem_dealloc(tmem, 256);
