@@ -175,3 +175,23 @@ def test_restated_sqd_matches_reference(name, ntype):
     np.testing.assert_allclose(q[m], g["q"][m], rtol=1e-5)
     scale = max(1.0, float(np.abs(g["sq"]).max()))
     assert np.abs(sq[m] - g["sq"][m]).max() < 1e-4 * scale
+
+
+def test_sqd_vector_set_is_a_half_space_within_the_cutoff():
+    """The restated G set holds exactly one of each +-G pair with 0 < |n|^2 <= (int)(q_max/g)^2, and
+    its bins follow |G| (the structure the device set-up also builds)."""
+    bl, nq, qmax = 18.624, 60, 6.0
+    ijk, gscl, b = orc.sqd_gvectors(bl, nq, qmax)
+    keys = {tuple(v) for v in ijk}
+    assert len(keys) == len(ijk)
+    assert not any(tuple(-v) in keys for v in ijk)
+    g = np.float32(np.float32(2 * np.pi) / np.float32(bl))
+    cut = int(np.float32(np.float32(qmax) / g) ** 2)
+    n2 = (ijk ** 2).sum(1)
+    assert n2.min() > 0 and n2.max() <= cut
+    r = np.arange(-int(np.float32(qmax) / g), int(np.float32(qmax) / g) + 1)
+    full = sum(1 for i in r for j in r for k in r if 0 < i * i + j * j + k * k <= cut)
+    assert 2 * len(ijk) == full
+    order = np.argsort(gscl, kind="stable")
+    assert np.all(np.diff(b[order]) >= 0)
+    assert b.min() >= 0 and b.max() <= nq - 1
