@@ -98,7 +98,7 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 // Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global memory into
-// this CTA's shared memory, counted on the barrier's transaction count. No multicast.
+// this CTA's shared memory, counted on the barrier's transaction count (a plain load, one destination CTA).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),
