@@ -38,7 +38,10 @@ enum {
   NNPE_DEV_GHOST_OVERFLOW = 2,  /* "ghost overflow", environ.cpp:440 */
   NNPE_DEV_CELL_RANGE = 4,      /* an atom or image outside the grid (CHECK_BINNING, environ.cpp:245-259) */
   NNPE_DEV_CELL_OVERFLOW = 8,   /* a cell holds more atoms than the in-cell sort supports */
-  NNPE_DEV_NAN = 16
+  NNPE_DEV_NAN = 16,
+  NNPE_DEV_TIMEOUT = 32,        /* a bounded wait on the tensor core gave up; the launch's results are void */
+  NNPE_DEV_POISONED = 64        /* a kernel that gave up could not see its own asynchronous copies land:
+                                   the context refuses further work (NNPE_ETIMEOUT) until nnpe_setup */
 };
 
 /* Per-log-step record of the step loop (run.cpp:376-392 prints the same quantities). */
@@ -163,13 +166,14 @@ int nnpe_compute_forces(nnpe_ctx* ctx, int ev, double* erg, double* virial);
  * to f_host (atom-id order); erg/virial (FP64) when non-NULL. */
 int nnpe_force_step(nnpe_ctx* ctx, const float* x_host, float* f_host, double* erg, double* virial);
 /* nnpe_force_step without any device allocation; no counterpart in the reference. Positions and
- * forces are staged in a statically reserved device array (3 MiB on every GPU that loads the
- * library, held until exit) instead of buffers allocated on first use, for callers that cannot let
- * the library allocate: a run loop whose process reserves the device's memory for its own
- * allocator, or one that cannot take the implicit inter-stream synchronisation of an allocation.
- * natom <= 131072, else NNPE_EARG. The first call on a device looks up the array's address with
- * that device current: make it before any stream capture. All contexts on a device share the
- * array, so calls that overlap in time race on it; serialise them. */
+ * forces are staged in a static device array (3 MiB) instead of buffers allocated on first use,
+ * for callers that cannot let the library allocate: a run loop whose process reserves the
+ * device's memory for its own allocator, or one that cannot take the implicit inter-stream
+ * synchronisation of an allocation. nnpe_setup resolves the array on the context's device (that
+ * loads the module holding it and reserves the 3 MiB there, until the process exits), so this
+ * call loads and reserves nothing; a device reset under a set-up context is not supported.
+ * natom <= 131072, else NNPE_EARG. All contexts on a device share the array, so calls that
+ * overlap in time race on it; serialise them. */
 int nnpe_force_step_noalloc(nnpe_ctx* ctx, const float* x_host, float* f_host, double* erg, double* virial);
 /* Forces (kind 0) or accelerations after the last step (kind 1), atom-id order [natom*3]. */
 int nnpe_get_forces(nnpe_ctx* ctx, int kind, float* f);

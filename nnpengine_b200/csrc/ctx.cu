@@ -406,8 +406,10 @@ int nnpe_setup(nnpe_ctx* c, double pair_cutoff, double skin, double gr_cutoff, i
   int ctrl[CTRL_WORDS] = {0};
   ctrl[CTRL_REBUILD] = 1;   // x_prev=INFINITY makes the first isvalid() false (neighlist.cpp:29)
   NNPE_CUDA(c, cudaMemcpy(c->d_ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice));
+  TRY(noalloc_stage_prepare(c));
   c->have_setup = true;
   c->first_step_done = false;
+  c->poisoned = false;
   return NNPE_OK;
 }
 

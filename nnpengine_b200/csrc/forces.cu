@@ -543,20 +543,22 @@ __global__ void k_qm_to_pos(const float2* __restrict__ qm, float4* __restrict__ 
 // Force evaluation at caller-owned host positions: the drop-in call a host-side run loop makes
 // (positions in, forces and energy out, in atom-id order). The list is checked and rebuilt on the
 // device as needed (run.cpp:236-283), then the force block runs (run.cpp:302-342).
-extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial) {
-  if (!c || !c->have_setup || !x_host || !f_host) return nnpe_fail(c, NNPE_EARG, "nnpe_force_step");
-  cudaSetDevice(c->device);
+int refuse_if_poisoned(nnpe_ctx* c) {
+  if (c->poisoned)
+    return nnpe_fail(c, NNPE_ETIMEOUT, "a device wait gave up with copies in flight: the context refuses work until nnpe_setup");
+  return 0;
+}
+
+int force_step_staged(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial, float* xstage,
+                      float* fstage) {
+  if (int rc = refuse_if_poisoned(c)) return rc;
   const int N = c->natom;
-  if (!c->d_xstage) {
-    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_xstage, sizeof(float) * 3 * N));
-    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_fstage, sizeof(float) * 3 * N));
-  }
   if (!c->first_step_done && !c->force_step_init) {
     k_qm_to_pos<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_qm, c->d_pos, N);
     c->force_step_init = true;
   }
-  NNPE_CUDA(c, cudaMemcpyAsync(c->d_xstage, x_host, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, c->stream));
-  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_xstage, c->d_atom_id, c->d_xd, c->d_pos, N, (double)c->grid.bl, c->fp64_state);
+  NNPE_CUDA(c, cudaMemcpyAsync(xstage, x_host, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, c->stream));
+  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(xstage, c->d_atom_id, c->d_xd, c->d_pos, N, (double)c->grid.bl, c->fp64_state);
   if (int rc = check_valid_enqueue(c)) return rc;
   if (int rc = rebuild_enqueue(c, true)) return rc;
   if (int rc = ghost_update_enqueue(c, true)) return rc;
@@ -566,8 +568,8 @@ extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, 
     if (int rc = energy_reduce_enqueue(c, 0)) return rc;
     NNPE_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
   }
-  k_gather_forces<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_frc, c->d_atom_id, c->d_fstage, N);
-  NNPE_CUDA(c, cudaMemcpyAsync(f_host, c->d_fstage, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, c->stream));
+  k_gather_forces<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_frc, c->d_atom_id, fstage, N);
+  NNPE_CUDA(c, cudaMemcpyAsync(f_host, fstage, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
   if (ev) {
     if (erg) *erg = c->h_red[0];
@@ -576,8 +578,20 @@ extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, 
   return NNPE_OK;
 }
 
+extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial) {
+  if (!c || !c->have_setup || !x_host || !f_host) return nnpe_fail(c, NNPE_EARG, "nnpe_force_step");
+  cudaSetDevice(c->device);
+  const int N = c->natom;
+  if (!c->d_xstage) {
+    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_xstage, sizeof(float) * 3 * N));
+    NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_fstage, sizeof(float) * 3 * N));
+  }
+  return force_step_staged(c, x_host, f_host, erg, virial, c->d_xstage, c->d_fstage);
+}
+
 extern "C" int nnpe_compute_forces(nnpe_ctx* c, int ev, double* erg, double* virial) {
   if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_compute_forces: not set up");
+  if (int rc = refuse_if_poisoned(c)) return rc;
   cudaSetDevice(c->device);
   if (int rc = forces_enqueue(c, ev != 0)) return rc;
   if (ev) {

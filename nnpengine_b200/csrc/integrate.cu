@@ -231,6 +231,7 @@ static int step_variant(nnpe_ctx* c, int md_step, int log_interval) {
 
 static int prepare_run(nnpe_ctx* c, int max_log) {
   if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_run: not set up");
+  if (int rc = refuse_if_poisoned(c)) return rc;
   if (!c->d_table && !c->nnp && c->pair_on) return nnpe_fail(c, NNPE_EARG, "nnpe_run: no pair table");
   cudaSetDevice(c->device);
   if (max_log > c->log_cap) {

@@ -68,6 +68,7 @@ struct nnpe_ctx {
   std::vector<int> top_bonds, top_angles, top_dihs;   // expanded topology read with the system
   // ---- setup ----
   bool have_system = false, have_setup = false, first_step_done = false;
+  bool poisoned = false;   // NNPE_DEV_POISONED seen: no further work until nnpe_setup
   float pair_cutoff = 10, skin = 2, gr_cutoff = 10, comm_cutoff = 12;
   int cap = 2048;
   GridParams grid{};
@@ -220,6 +221,15 @@ int gr_tally_enqueue(nnpe_ctx* c, int inner);
 int alloc_state(nnpe_ctx* c);
 int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
 int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6 = true);
+// The host-positions force step (nnpe_force_step) with its staging buffers given by the caller:
+// xstage and fstage hold at least 3 * natom floats each on the context's device.
+int force_step_staged(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial, float* xstage,
+                      float* fstage);
+// Resolves the device address of the allocation-free step's static staging on c's device (loading
+// the module that holds it); nnpe_setup calls it so that later steps load and reserve nothing.
+int noalloc_stage_prepare(nnpe_ctx* c);
+// A context that saw NNPE_DEV_POISONED refuses work until nnpe_setup.
+int refuse_if_poisoned(nnpe_ctx* c);
 int nnpe_bonded_coefs(nnpe_ctx* c, const float* bcoef, const float* acoef, const float* dcoef);
 void nnp_free(nnpe_ctx* c);
 // Device allocations of a context go through these two, which keep the context's byte count

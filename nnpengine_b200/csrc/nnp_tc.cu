@@ -33,8 +33,6 @@
 #include "nnp.cuh"
 #include "tc_util.cuh"
 
-#define NNPE_DEV_TIMEOUT 32
-
 struct NnpTc {
   unsigned long long* d_facc = nullptr;   // network forces and virial [natom][4], fixed point (2^-32)
   unsigned char* d_fit = nullptr;    // per species: L1 (N128,K256) L2 (128,128) B2 (128,128) B1 (256,128)
@@ -865,8 +863,12 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   if (!ok && t == 0) {
     // a wait gave up: let the bulk loads still in flight land (bounded) before the CTA exits. A
     // buffer's phases complete in order, so waiting for the parity of its last load covers both.
-    if (issued0) tc::mbar_wait(&bar_w[0], (uint32_t)((issued0 - 1) & 1), 200000000ll);
-    if (issued1) tc::mbar_wait(&bar_w[1], (uint32_t)((issued1 - 1) & 1), 200000000ll);
+    // If that wait gives up too, copies may still land in shared memory that the SM hands to the
+    // next CTA: the context is poisoned and the host refuses further work on it.
+    bool drained = true;
+    if (issued0) drained = tc::mbar_wait(&bar_w[0], (uint32_t)((issued0 - 1) & 1), 200000000ll) && drained;
+    if (issued1) drained = tc::mbar_wait(&bar_w[1], (uint32_t)((issued1 - 1) & 1), 200000000ll) && drained;
+    if (!drained) atomicOr(f.ctrl + CTRL_ERR, NNPE_DEV_POISONED);
   }
   tc::fence_before();
   __syncthreads();

@@ -372,6 +372,10 @@ static int sync_errors(nnpe_ctx* c) {
   NNPE_CUDA(c, cudaMemcpyAsync(c->h_ctrl, c->d_ctrl, sizeof(int) * CTRL_WORDS, cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
   const int e = c->h_ctrl[CTRL_ERR];
+  if (e & NNPE_DEV_POISONED) c->poisoned = true;
+  if (c->poisoned)
+    return nnpe_fail(c, NNPE_ETIMEOUT, "a device wait gave up with copies in flight: the context refuses work until nnpe_setup");
+  if (e & NNPE_DEV_TIMEOUT) return nnpe_fail(c, NNPE_ETIMEOUT, "a bounded device wait gave up");
   if (e & NNPE_DEV_LIST_OVERFLOW) return nnpe_fail(c, NNPE_EOVERFLOW, "nei_list overflow");
   if (e & NNPE_DEV_GHOST_OVERFLOW) return nnpe_fail(c, NNPE_EOVERFLOW, "ghost overflow");
   if (e & NNPE_DEV_CELL_OVERFLOW) return nnpe_fail(c, NNPE_EOVERFLOW, "cell overflow in sort");

@@ -28,11 +28,18 @@ def _step(e, fn, x):
     return rc, f, erg.value, vir.value
 
 
+def _device_bytes(e):
+    b = C.c_int64(0)
+    assert e.lib.nnpe_device_bytes(e.h, C.byref(b)) == 0
+    return b.value
+
+
 def test_force_step_noalloc_matches_force_step():
     s, table = cases.water_case(jitter=0.05)
     ref, stat = _engine(s, table), _engine(s, table)
     x1 = np.ascontiguousarray(s.x, np.float32)
     x2 = (x1 + np.random.default_rng(11).normal(0, 0.02, x1.shape)).astype(np.float32)
+    bytes_before = _device_bytes(stat)
     for x in (x1, x2):   # two calls in a row on each context
         rc_a, fa, ea, va = _step(ref, ref.lib.nnpe_force_step, x)
         rc_b, fb, eb, vb = _step(stat, stat.lib.nnpe_force_step_noalloc, x)
@@ -41,6 +48,10 @@ def test_force_step_noalloc_matches_force_step():
         np.testing.assert_array_equal(fa, fb)
         assert ea == eb and va == vb
         assert np.abs(fb).max() > 0
+    # the point of the entry point: the context's device-byte ledger did not move, while the
+    # allocating step's context grew by its two staging buffers
+    assert _device_bytes(stat) == bytes_before
+    assert _device_bytes(ref) >= bytes_before + 2 * 4 * 3 * s.natom
 
 
 def test_force_step_noalloc_rejects_systems_over_its_limit():
