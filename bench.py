@@ -29,21 +29,25 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 WORKLOADS = {
-    "water96k-nnp-bf16": dict(n_side=32, bl=99.3, nmol=32000, nnp="bf16",
+    "water96k-nnp-bf16": dict(n_side=32, bl=99.3, nmol=32000, nnp="bf16", cpu_steps=2,
                               desc="96,000-atom water (32,000 molecules, 99.3 A box): tabulated LJ + DSF Coulomb at 10 A "
                                    "plus the radial-embedding network at 6 A (1->32->64 per species, 4 special-class "
                                    "slots, fitting 256->128->128->1, tanh) with BF16 tcgen05 GEMMs and FP32 accumulation; "
                                    "2 A skin, bonds + angles, dt 0.5 fs NVE, FP64 Verlet state"),
-    "water96k-nnp-fp32": dict(n_side=32, bl=99.3, nmol=32000, nnp="fp32",
+    "water96k-nnp-tbl": dict(n_side=32, bl=99.3, nmol=32000, nnp="tbl", cpu_steps=2,
+                             desc="the reference's own tabulated NNP on the 96,000-atom water box: NNPOTENTIAL_TBL at 6 A "
+                                  "(20 Gaussian descriptors per special class, 20->128->128->1 tanh fitting network in "
+                                  "FP32, its pair tables) plus LJ/DSF at 10 A and bonds + angles, dt 0.5 fs NVE"),
+    "water96k-nnp-fp32": dict(n_side=32, bl=99.3, nmol=32000, nnp="fp32", cpu_steps=2,
                               desc="the same 96,000-atom NNP + tabulated workload with the network in FP32 on CUDA cores "
                                    "(the plain form)"),
-    "water96k-classical": dict(n_side=32, bl=99.3, nmol=32000, nnp=None,
+    "water96k-classical": dict(n_side=32, bl=99.3, nmol=32000, nnp=None, cpu_steps=20,
                                desc="96,000-atom water (32,000 molecules, 99.3 A box), tabulated LJ + DSF Coulomb at "
                                     "10 A, 2 A skin, bonds + angles, dt 0.5 fs NVE, FP64 Verlet state"),
-    "water3k-classical": dict(n_side=10, bl=31.04, nmol=None, nnp=None,
+    "water3k-classical": dict(n_side=10, bl=31.04, nmol=None, nnp=None, cpu_steps=400,
                               desc="3,000-atom water (1,000 molecules, 31.04 A box), tabulated LJ + DSF Coulomb at 10 A, "
                                    "2 A skin, bonds + angles, dt 0.5 fs NVE"),
-    "gr-refine-30k": dict(mixture=True, natom=30000, rho=0.035, nnp=None,
+    "gr-refine-30k": dict(mixture=True, natom=30000, rho=0.035, nnp=None, cpu_steps=20,
                           desc="g(r)/S(q) refinement: 30,000-atom two-species LJ + DSF Coulomb liquid (60/40, sigma "
                                "3.0/3.4 A, eps 0.15/0.25 kcal/mol, charges +-0.5 e) at 0.035 A^-3 (94.99 A box); g(r) "
                                "to 15 A in 0.01 A bins (uint64 counts) every step (cell-based every 10), S(q) on 512 "
@@ -172,26 +176,51 @@ def make_engine(s, table, device, nnp=None):
     e.set_pair_table(F, U)
     if not mixture:
         e.set_bonded(s, [E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)], [E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)])
-    if nnp:
+    if nnp == "tbl":   # the reference's tabulated NNP, from its paramfile and weight file
+        with tempfile.TemporaryDirectory() as d:
+            paths = cases.write_nnp_inputs(NM.gauss_model(h1=128, h2=128), d)
+            e.nnp_load(6.0, 750, paths["param"], paths["wt"])
+    elif nnp:
         e.nnp_set(NM.embed_model(), 6.0, 750)
         e.nnp_precision(nnp == "bf16")
     return e
 
 
+def ref_layouts():
+    """The reference harness's two thread layouts: its default 3x3x3 = 27 threads as it runs
+    (unbound), and its 2x2x2 = 8-thread layout bound one thread per core (OMP_PROC_BIND=close,
+    OMP_PLACES=cores)."""
+    return [(27, {}), (8, {"OMP_PROC_BIND": "close", "OMP_PLACES": "cores"})]
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_reference(wl, steps: int):
-    """The reference's own OpenMP force step on the same system (oracle/_ref/ref_dump_fast): its
+    """The reference's own OpenMP force step on the same system (oracle/_ref/ref_dump_fast*): its
     LJTableCoulDSF + bonded terms, and for network workloads its tabulated NNP (NNPOTENTIAL_TBL at
-    6 A with a 20->128->128->1 fitting network behind the TF C-API shim; the reference cannot run
-    the embedding network). Timed over its MD loop only; returns (atom-steps/s, threads, sample)."""
+    6 A, 20 Gaussians per special class, with a 20->128->128->1 float fitting network behind the TF
+    C-API shim, serial as the reference configures TF; the reference cannot run the embedding
+    network). The MD loop runs `steps` and 2*`steps` steps; the rate is natom*steps over the
+    difference of the two loop times, so that set-up and the first list build cancel. Both thread
+    layouts run; the faster gives the value. Returns (atom-steps/s, threads, sample, details)."""
     from oracle import orc
     import cases
     from nnpengine_b200 import nnp_model as NM
     s, table = build_system(wl)
+    details = []
     with tempfile.TemporaryDirectory() as d:
         f = cases.write_inputs(s, table, d)
         cfg = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10,
                "bond": [f"1.0 {cases.WATER_BOND_K}"], "angle": [f"109.47 0 0 {cases.WATER_ANGLE_KC}"],
-               "velocity": f["vel"], "mode": "md", "steps": steps, "dt": 0.5, "log_interval": steps}
+               "velocity": f["vel"], "mode": "md", "dt": 0.5}
         what = "LJ/DSF table + bonded"
         if wl.get("mixture"):
             from nnpengine_b200 import systems as S
@@ -204,14 +233,24 @@ def cpu_reference(wl, steps: int):
         if wl.get("nnp"):
             paths = cases.write_nnp_inputs(NM.gauss_model(h1=128, h2=128), d)
             cfg["nnp"] = f"6.0 750 {paths['param']} {paths['wt']}"
-            what += " + its tabulated NNP (20 Gaussians/slot, 20->128->128->1 net via the C-API shim)"
-        out = orc.run_ref_dump(cfg, os.path.join(d, "o"), fast=True, timeout=1800)
-    t = float(out["info"]["t_loop"])
-    n = steps + 1   # md_step = 0..steps inclusive
+            what += (" + its tabulated NNP (20 Gaussians per special class, 20->128->128->1 float network via the "
+                     "C-API shim, serial as the reference configures TF)")
+        for threads, envx in ref_layouts():
+            env = dict(os.environ, **envx)
+            t = []
+            for n in (steps, 2 * steps):
+                out = orc.run_ref_dump({**cfg, "steps": n, "log_interval": n}, os.path.join(d, f"o{threads}_{n}"),
+                                       fast=True, timeout=1800, threads=threads, env=env)
+                t.append(float(out["info"]["t_loop"]))
+            dt = max(t[1] - t[0], 1e-9)
+            details.append({"threads": threads, "env": envx, "loop_s": t, "steps": [steps, 2 * steps],
+                            "atom_steps_per_s": s.natom * steps / dt})
+    best = max(details, key=lambda r: r["atom_steps_per_s"])
     ncpu = os.cpu_count()
-    return (s.natom * n / t, int(out["info"]["threads"]),
-            f"{n} MD steps of the {s.natom}-atom system ({what}), MD loop only, {out['info']['threads']} OpenMP "
-            f"threads on a {ncpu}-CPU host")
+    sample = (f"{s.natom}-atom system ({what}); MD loop of {steps} and {2 * steps} steps, rate from the difference; "
+              f"layouts 27 threads (3x3x3, unbound) and 8 threads (2x2x2, one per core), the faster reported; "
+              f"{ncpu}-CPU host ({cpu_model()})")
+    return best["atom_steps_per_s"], best["threads"], sample, details
 
 
 def cpu_sqd_reference(wl):
@@ -349,23 +388,13 @@ def serve_bench(args, wl):
 
 
 def refine_setup(e, s, wl, device, args):
-    """RMDF target: the weighted S(q) of the same liquid with every eps scaled by 1.1 after
-    `--target-steps` steps at 300 K (Andersen), computed by the library itself; then g(r) every step
-    (cell-based every 10) and RMDF with gamma 1 on the workload's engine."""
-    from nnpengine_b200 import systems as S
-    r, F11, U11 = S.lj_table(2, MIX_SIGMA, tuple(1.1 * x for x in MIX_EPS), 10.0, 1000)
-    et = make_engine(s, (r, F11, U11), device)
-    et.verlet(1.0, True)
-    et.thermostat("andersen", 300.0, 300.0, interval=1, frac=0.1, seed=21, total_steps=0)
-    et.gr_setup(1000, 512, 20.0)
-    et.run(args.target_steps, log_interval=args.target_steps, graph=True)
-    et.gr_tally(inner=False)
-    et.sq(False)
-    q, _, wt, ff = S.synthetic_sq_target(512, 20.0, 2)
-    et.rmdf_set(np.zeros((1, 512)), wt[None], ff[None], 0.0, 1.0)
-    et.rmdf_step()
-    target = et.rmdf_get()[0][0].copy()
-    et.close()
+    """RMDF target: the weighted S(q) that the reference itself computed (RMDF's sq, what
+    RMDF::dumpSQ writes) for the same 30,000-atom liquid with every eps scaled by 1.1, after 500
+    steps at 1 fs under its Andersen thermostat at 300 K (tests/golden/mixture30k.npz, written by
+    tests/golden/make_golden.py from oracle/_ref). Then g(r) every step (cell-based every 10) and
+    RMDF with gamma 1 on the workload's engine."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "mixture30k.npz"))
+    target, wt, ff = g["target_sq"].astype(np.float64), g["target_wt"], g["target_ff"]
     e.gr_setup(1000, 512, 20.0, gr_interval=1, gr_interval_long=10)
     e.rmdf_set(target[None], wt[None], ff[None], args.rmdf_strength, 1.0)
     return target
@@ -411,29 +440,123 @@ def time_enqueue(e, stream, which, reps):
     return a.elapsed_time(b) / reps
 
 
+def force_errors(s, table, x, device, m=None):
+    """Force and energy errors of the GPU forms against the FP64 oracle at positions x (float32,
+    atom-id order): the BF16 tensor-core network and the plain FP32 network, each as the network
+    term alone (6 A) and as the whole force (LJ/DSF at 10 A + bonded + network). Error = RMS of the
+    per-atom force difference over the RMS of the FP64 force; energies relative."""
+    import cases
+    from nnpengine_b200 import engine as E
+    from nnpengine_b200 import nnp_model as NM
+    from oracle import orc
+    m = m or NM.embed_model()
+    F, U = cases.table_as_loaded(table[1], table[2])
+    e = make_engine(s, table, device, "bf16")
+    e.set_positions(x)
+    e.set_velocities(np.zeros_like(x))
+    e.list_build()
+    got = {}
+    for prec in ("bf16", "fp32"):
+        e.nnp_precision(prec == "bf16")
+        erg, _ = e.compute_forces(True)
+        got[prec] = (e.forces().astype(np.float64), erg)
+    e.pair_enable(False)
+    e.set_bonded(s, [], [], [])
+    for prec in ("bf16", "fp32"):
+        e.nnp_precision(prec == "bf16")
+        erg, _ = e.compute_forces(True)
+        got[prec + "_net"] = (e.forces().astype(np.float64), erg)
+    errors = e.device_errors()
+    e.close()
+    sx = dataclass_replace_x(s, x)
+    o = orc.Restated(sx, "f64")
+    assert o.rebuild(x, 10, 2, 12) == 0
+    fp, ep, _ = o.pair_forces(F, U, 10.0)
+    fb, eb, _ = o.bonded(E.bond_coef(1.0, 0, 0, cases.WATER_BOND_K)[None],
+                         E.angle_coef(109.47, 0, 0, cases.WATER_ANGLE_KC)[None], np.zeros((1, 4), np.float32))
+    o6 = orc.Restated(sx, "f64")
+    assert o6.rebuild(x, 6, 2, 8) == 0
+    r = o6.nnp_emb(6.0, m.scale, m.e1, m.e2, m.embw, m.h1, m.h2, m.fitw)
+    ref_net, ref_tot = r["f"], fp + fb + r["f"]
+    e_net, e_tot = r["e_net"], ep + eb + r["e_net"]
+    out = {"oracle": "FP64 C restatement (oracle/restate) at the final state of the timed run", "natom": s.natom,
+           "device_error_bits": errors, "force_rms_fp64": {"network": float(np.sqrt((ref_net ** 2).sum(1).mean())),
+                                                           "total": float(np.sqrt((ref_tot ** 2).sum(1).mean()))}}
+    for prec in ("bf16", "fp32"):
+        out[prec] = {"force_rel_rmse_network": cases.rel_rms(got[prec + "_net"][0], ref_net),
+                     "force_rel_rmse_total": cases.rel_rms(got[prec][0], ref_tot),
+                     "energy_rel_err_network": abs(got[prec + "_net"][1] - e_net) / abs(e_net),
+                     "energy_rel_err_total": abs(got[prec][1] - e_tot) / abs(e_tot)}
+    out["bar"] = "BF16: force RMSE <= 1% of the FP64 force RMS; FP32: 1e-5 force, 1e-6 energy"
+    return out
+
+
+def dataclass_replace_x(s, x):
+    import dataclasses
+    return dataclasses.replace(s, x=np.asarray(x, np.float32).reshape(-1, 3))
+
+
+def same_model_gpu(s, table, x, v, device, steps, warmup=10):
+    """The reference's own tabulated NNP (the model its CPU path runs: 20 Gaussians per special
+    class, 20->128->128->1, read from the reference-format paramfile and weight file) plus LJ/DSF
+    and bonded terms on the GPU (FP32 network on CUDA cores), NVE at 0.5 fs from state (x, v);
+    atom-steps/s over `steps` graph-replayed steps (CUDA events on the library's stream)."""
+    import torch
+    e = make_engine(s, table, device, "tbl")
+    e.set_positions(x)
+    e.set_velocities(v)
+    e.verlet(0.5, True)
+    e.run(warmup, log_interval=warmup, graph=True)
+    stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    e.run(steps, log_interval=steps, graph=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    e.close()
+    return s.natom / (ms / 1e3), ms
+
+
+def reference_workload(name):
+    """The workload the reference's CPU path runs for a GPU workload: the same system; for the
+    embedding network (which the reference cannot run) its own tabulated NNP; for serving one
+    3000-atom replica."""
+    wl = WORKLOADS[name]
+    if wl.get("serve"):
+        return WORKLOADS["water3k-classical"] | {"nnp": "bf16", "cpu_steps": 10}
+    return wl
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=0, help="timed steps (0: 2000 for gr-refine-30k, the configured "
+                    "refinement length, else 1000)")
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="water96k-nnp-bf16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the plain FP32 network alongside")
+    ap.add_argument("--no-errors", action="store_true", help="skip the FP64 force-error evaluation")
+    ap.add_argument("--no-same-model", action="store_true", help="skip the GPU run of the reference's own model")
     ap.add_argument("--exact", action="store_true", help="pair forces in the reference's exact float sequence")
     ap.add_argument("--no-autotune", action="store_true", help="default grids for the tensor-core kernels")
-    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--cpu-steps", type=int, default=0, help="reference MD-loop sample: N and 2N steps (0: per workload)")
     ap.add_argument("--equil", type=int, default=5000)
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-scale", type=float, default=1.0, help="multiply every request's step count")
     ap.add_argument("--serve-slots", type=int, default=64)
     ap.add_argument("--serve-timeout", type=float, default=900.0)
-    ap.add_argument("--drift-ps", type=float, default=0.0, help="after the timed steps, NVE for this many ps")
-    ap.add_argument("--target-steps", type=int, default=500)
+    ap.add_argument("--drift-ps", type=float, default=-1.0,
+                    help="after the timed steps, NVE for this many ps (-1: 10 ps for the network workloads)")
     ap.add_argument("--rmdf-strength", type=float, default=0.02)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.steps <= 0:
+        args.steps = 2000 if wl.get("mixture") else 1000
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -442,15 +565,23 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cwl = (WORKLOADS["water3k-classical"] | {"nnp": "bf16"}) if wl.get("serve") else wl
+        rwl = reference_workload(args.workload)
         unit = "atom-G evaluations/s" if wl.get("sqd") else "atom-steps/s"
-        rate, threads, sample = cpu_sqd_reference(wl) if wl.get("sqd") else cpu_reference(cwl, args.cpu_steps)
+        details = None
+        if wl.get("sqd"):
+            rate, threads, sample = cpu_sqd_reference(wl)
+        else:
+            rate, threads, sample, details = cpu_reference(rwl, args.cpu_steps or rwl.get("cpu_steps", 20))
+        cfg = {"workload": args.workload, "description": wl["desc"]}
+        if wl.get("nnp") == "bf16" or wl.get("serve"):
+            cfg["model"] = ("the reference's own tabulated NNP (it cannot run the embedding network of this "
+                            "workload); the GPU on this same model is the 'same_model' block of the GPU arm's line")
         print(json.dumps({
             "impl": "reference", "metric": unit, "value": rate, "unit": unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "description": wl["desc"]},
-            "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "reference", "sample": sample},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": cfg,
+            "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "reference", "sample": sample,
+                             "layouts": details},
             "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
@@ -485,9 +616,11 @@ def main():
         cpu = None
         if not args.no_cpu_baseline:
             try:
-                rate, threads, sample = cpu_reference(WORKLOADS["water3k-classical"] | {"nnp": "bf16"}, args.cpu_steps)
+                rwl = reference_workload(args.workload)
+                rate, threads, sample, details = cpu_reference(rwl, args.cpu_steps or rwl["cpu_steps"])
                 cpu = {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
-                       "sample": sample + "; the reference runs one system per process, so a stream is sequential runs"}
+                       "sample": sample + "; the reference runs one system per process, so a stream is sequential runs",
+                       "layouts": details}
             except Exception as ex:
                 cpu = {"value": None, "unit": "atom-steps/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {ex}"}
         print(json.dumps({
@@ -559,8 +692,9 @@ def main():
     x_e2e0, v_e2e0 = e.positions().astype(np.float32), e.velocities().astype(np.float32)
 
     drift = None
-    if args.drift_ps > 0 and not refine:
-        drift = nve_drift(e, s.natom, args.drift_ps)
+    drift_ps = args.drift_ps if args.drift_ps >= 0 else (10.0 if wl.get("nnp") else 0.0)
+    if drift_ps > 0 and not refine:
+        drift = nve_drift(e, s.natom, drift_ps)
 
     plain = None
     if wl.get("nnp") == "bf16" and not args.no_compare:
@@ -587,7 +721,7 @@ def main():
         kms["network"] = time_enqueue(e, stream, 3, reps)
     hbm, bf16, bf16s, src = peaks()
     nlist = info["entries"] / s.natom
-    if wl.get("nnp"):
+    if wl.get("nnp") in ("bf16", "fp32"):
         # network pairs inside 6 A from the compact list of the last evaluation
         G, dG, ea = e.nnp_get()
         pairs6 = int(e.lib.nnpe_nnp_pairs(e.h))
@@ -614,7 +748,21 @@ def main():
         gr_info = {"ordered_pairs_per_cell_tally": ordered,
                    "cell_tally_pair_evaluations_per_s": ordered / (kms["gr_cell"] / 1e3),
                    "rmdf_penalty_first_last": [exp[0], exp[-1]] if exp else None, "rmdf_strength": args.rmdf_strength,
-                   "target": "weighted S(q) of the eps x1.1 liquid after %d steps (library-computed)" % args.target_steps}
+                   "target": "weighted S(q) of the eps x1.1 liquid after 500 steps under the reference's Andersen thermostat, "
+                             "computed by the reference (oracle/_ref, RMDF's sq)"}
+
+    # the stated error of the timed state against the FP64 oracle, and the GPU on the reference's
+    # own model (rank 0; no collective inside either)
+    errs = None
+    if wl.get("nnp") == "bf16" and not args.no_errors and rank == 0:
+        errs = force_errors(s, table, x_e2e0, local)
+    same = None
+    if wl.get("nnp") == "bf16" and not args.no_same_model and rank == 0:
+        nsm = max(20, min(200, args.steps))
+        rate_g, ms_g = same_model_gpu(s, table, x_e2e0, v_e2e0, local, nsm)
+        same = {"workload": "water96k-nnp-tbl", "description": WORKLOADS["water96k-nnp-tbl"]["desc"],
+                "gpu_value": rate_g, "gpu_ms_per_step": ms_g, "gpu_steps": nsm, "unit": "atom-steps/s",
+                "reference_value": None, "gpu_over_reference": None}
 
     e2e = None
     if not args.no_e2e:
@@ -649,8 +797,13 @@ def main():
         cpu = None
         if not args.no_cpu_baseline:
             try:
-                rate, threads, sample = cpu_reference(wl, args.cpu_steps)
-                cpu = {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference", "sample": sample}
+                rwl = reference_workload(args.workload)
+                rate, threads, sample, details = cpu_reference(rwl, args.cpu_steps or rwl.get("cpu_steps", 20))
+                cpu = {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference", "sample": sample,
+                       "layouts": details}
+                if same is not None:
+                    same["reference_value"] = rate
+                    same["gpu_over_reference"] = same["gpu_value"] / rate
             except Exception as ex:  # the reference harness is optional on a box without it
                 cpu = {"value": None, "unit": "atom-steps/s", "cores": 0, "kind": "reference",
                        "sample": f"unavailable: {ex}"}
@@ -668,6 +821,10 @@ def main():
             cfg["gr_refinement"] = gr_info
         if drift is not None:
             cfg["nve_drift"] = drift
+        if errs is not None:
+            cfg["force_error_vs_fp64"] = errs
+        if same is not None:
+            cfg["same_model"] = same
         out = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

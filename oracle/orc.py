@@ -20,12 +20,21 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _libs: Dict[str, C.CDLL] = {}
 
 
+# Where the reference's sources are read from (the only place that names it; REFSRC overrides it).
+REFSRC_DEFAULT = "/root/reference/src"
+
+
+def refsrc() -> str:
+    return os.environ.get("REFSRC", REFSRC_DEFAULT)
+
+
 def build(quiet: bool = True) -> None:
     """Compile the restatement (always) and the reference harness (when its sources exist)."""
     targets = ["restate"]
-    if os.path.isdir(os.environ.get("REFSRC", "/root/reference/src")):
+    src = refsrc()
+    if os.path.isdir(src):
         targets.append("ref")
-    subprocess.run(["make", "-C", HERE, "-j8"] + targets, check=True,
+    subprocess.run(["make", "-C", HERE, "-j8", f"REFSRC={src}"] + targets, check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
 
@@ -162,8 +171,10 @@ def ref_available() -> bool:
 
 
 def run_ref_dump(cfg: Dict[str, str], workdir: str, fast: bool = False, env: Optional[dict] = None,
-                 timeout: float = 600) -> Dict[str, np.ndarray]:
-    """Write ``cfg`` (key -> value text) and run the reference harness; returns its arrays."""
+                 timeout: float = 600, threads: int = 27) -> Dict[str, np.ndarray]:
+    """Write ``cfg`` (key -> value text) and run the reference harness; returns its arrays.
+    fast: the timing build (-O3 AVX2, float network in the shim); threads: 27 (the reference's
+    3x3x3 layout) or 8 (its 2x2x2 layout), timing build only."""
     os.makedirs(workdir, exist_ok=True)
     cfg = dict(cfg)
     cfg.setdefault("out", workdir)
@@ -175,7 +186,9 @@ def run_ref_dump(cfg: Dict[str, str], workdir: str, fast: bool = False, env: Opt
                     f.write(f"{k} {item}\n")
             else:
                 f.write(f"{k} {v}\n")
-    exe = os.path.join(REF_DIR, "ref_dump_fast" if fast else "ref_dump")
+    if threads not in (27, 8) or (threads == 8 and not fast):
+        raise ValueError("the harness is built for 27 threads, and for 8 in its timing build")
+    exe = os.path.join(REF_DIR, ("ref_dump_fast8" if threads == 8 else "ref_dump_fast") if fast else "ref_dump")
     subprocess.run([exe, path], check=True, cwd=workdir, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                    env=env, timeout=timeout)
     return read_ref_dump(workdir)

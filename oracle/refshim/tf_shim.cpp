@@ -31,6 +31,9 @@ struct FitNet {
   int din = 0, h1 = 0, h2 = 0, ntype = 0;
   std::vector<int> slot_type;           // per atom slot of the molecule
   std::vector<std::vector<double>> A1, c1, A2, c2, A3, c3;  // per type
+  // float copies for the timing build (TF evaluates the reference's network in float): the
+  // weights as read and transposed, so that every loop below runs along contiguous memory
+  std::vector<std::vector<float>> fA1, fc1, fA2, fc2, fA3, fA1T, fA2T;
 };
 }  // namespace
 
@@ -99,6 +102,18 @@ TF_Session* TF_LoadSessionFromSavedModel(const TF_SessionOptions*, const TF_Buff
          rd(n.c2[t], n.h2) && rd(n.A3[t], n.h2) && rd(n.c3[t], 1);
   fclose(fp);
   if (!ok) { delete sess; set_status(st, TF_INVALID_ARGUMENT, "truncated model weights"); return nullptr; }
+  n.fA1.resize(n.ntype); n.fc1.resize(n.ntype); n.fA2.resize(n.ntype); n.fc2.resize(n.ntype);
+  n.fA3.resize(n.ntype); n.fA1T.resize(n.ntype); n.fA2T.resize(n.ntype);
+  for (int t = 0; t < n.ntype; ++t) {
+    n.fA1[t].assign(n.A1[t].begin(), n.A1[t].end()); n.fc1[t].assign(n.c1[t].begin(), n.c1[t].end());
+    n.fA2[t].assign(n.A2[t].begin(), n.A2[t].end()); n.fc2[t].assign(n.c2[t].begin(), n.c2[t].end());
+    n.fA3[t].assign(n.A3[t].begin(), n.A3[t].end());
+    n.fA1T[t].resize((size_t)n.din * n.h1); n.fA2T[t].resize((size_t)n.h1 * n.h2);
+    for (int d = 0; d < n.din; ++d)
+      for (int k = 0; k < n.h1; ++k) n.fA1T[t][(size_t)k * n.din + d] = (float)n.A1[t][(size_t)d * n.h1 + k];
+    for (int k = 0; k < n.h1; ++k)
+      for (int m = 0; m < n.h2; ++m) n.fA2T[t][(size_t)m * n.h1 + k] = (float)n.A2[t][(size_t)k * n.h2 + m];
+  }
   set_status(st, TF_OK, "");
   g_last_session = sess;
   return sess;
@@ -135,6 +150,55 @@ void TF_SessionRun(TF_Session* session, const TF_Buffer*, const TF_Output*, TF_T
   float* dG = (float*)tD->data.data();
   double E = 0;
   const int nslot = (int)n.slot_type.size();
+#ifdef SHIM_FLOAT
+  // Timing build: the network in float, as TF runs the reference's model, serial, as the
+  // reference configures its TF session (intra/inter-op threads 1, pair_nnp.cpp:23-24); every
+  // inner loop runs along contiguous weights so that the compiler vectorises it.
+  {
+    std::vector<float> h1(n.h1), h2(n.h2), g1(n.h1), g2(n.h2);
+    for (long a = 0; a < (long)natom; ++a) {
+      const int t = n.slot_type[a % nslot];
+      const float* g = G + a * n.din;
+      const float *A1 = n.fA1[t].data(), *c1 = n.fc1[t].data(), *A2 = n.fA2[t].data(), *c2 = n.fc2[t].data();
+      const float *A3 = n.fA3[t].data(), *A1T = n.fA1T[t].data(), *A2T = n.fA2T[t].data();
+      for (int k = 0; k < n.h1; ++k) h1[k] = c1[k];
+      for (int d = 0; d < n.din; ++d) {
+        const float gd = g[d];
+        const float* row = A1 + (size_t)d * n.h1;
+        for (int k = 0; k < n.h1; ++k) h1[k] += gd * row[k];
+      }
+      for (int k = 0; k < n.h1; ++k) h1[k] = std::tanh(h1[k]);
+      for (int m = 0; m < n.h2; ++m) h2[m] = c2[m];
+      for (int k = 0; k < n.h1; ++k) {
+        const float hk = h1[k];
+        const float* row = A2 + (size_t)k * n.h2;
+        for (int m = 0; m < n.h2; ++m) h2[m] += hk * row[m];
+      }
+      float e = (float)n.c3[t][0];
+      for (int m = 0; m < n.h2; ++m) {
+        h2[m] = std::tanh(h2[m]);
+        e += h2[m] * A3[m];
+        g2[m] = A3[m] * (1 - h2[m] * h2[m]);
+      }
+      E += e;
+      for (int k = 0; k < n.h1; ++k) g1[k] = 0;
+      for (int m = 0; m < n.h2; ++m) {
+        const float gm = g2[m];
+        const float* row = A2T + (size_t)m * n.h1;
+        for (int k = 0; k < n.h1; ++k) g1[k] += gm * row[k];
+      }
+      for (int k = 0; k < n.h1; ++k) g1[k] *= 1 - h1[k] * h1[k];
+      float* out = dG + a * n.din;
+      for (int d = 0; d < n.din; ++d) out[d] = 0;
+      for (int k = 0; k < n.h1; ++k) {
+        const float gk = g1[k];
+        const float* row = A1T + (size_t)k * n.din;
+        for (int d = 0; d < n.din; ++d) out[d] += gk * row[d];
+      }
+    }
+  }
+  if (false)
+#endif
   // serial, as the reference configures its TF session (intra/inter-op threads 1, pair_nnp.cpp:23-24)
   for (long a = 0; a < (long)natom; ++a) {
     std::vector<double> h1(n.h1), h2(n.h2), g1(n.h1), g2(n.h2);

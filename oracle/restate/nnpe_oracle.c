@@ -670,61 +670,76 @@ int orc_nnp_emb(const orc_t* o, double cutoff_d, double scale_d, int e1, int e2,
   const size_t eb = (size_t)e1 + e1 + (size_t)e1 * e2 + e2;
   real* G = (real*)calloc((size_t)N * din, sizeof(real));
   real* dG = (real*)calloc((size_t)N * din, sizeof(real));
-  real* h = (real*)malloc(sizeof(real) * (e1 + e2 + e1));
-  real *t = h + e1 + e2;
-  for (int i = 0; i < N; ++i) {
-    const int ia = o->order[i];
-    const real* xi = o->xs + 3 * i;
-    for (long k = o->lstart[i]; k < o->lstart[i + 1]; ++k) {
-      const int j = o->lj[k], ja = o->order[j];
-      const real* xj = o->xs + 3 * j;
-      real rsq = sqr(xi[0] - xj[0]) + sqr(xi[1] - xj[1]) + sqr(xi[2] - xj[2]);
-      if (!(rsq < cutsq)) continue;
-      real r = sqrt(rsq), u = r * r_rc;
-      int s = special_of(o, ia, ja);
-      const float *W1 = embw + eb * o->typ[ja], *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
-      real cf = r - rc, cff = 1 - 1 / (1 + cf * cf);
-      for (int a = 0; a < e1; ++a) h[a] = tanh((real)W1[a] * u + (real)b1[a]);
-      for (int c = 0; c < e2; ++c) {
-        real z = (real)b2[c];
-        for (int a = 0; a < e1; ++a) z += h[a] * (real)W2[(size_t)a * e2 + c];
-        G[(size_t)ia * din + s * e2 + c] += scale * tanh(z) * cff;
+  double* ea_all = (double*)calloc((size_t)N, sizeof(double));
+  double* w_all = (double*)calloc((size_t)N, sizeof(double));
+  /* Each loop writes only the rows of its own atom i and sums them in list order, and the
+   * energy and virial are summed over atoms serially afterwards: the result does not depend on
+   * the thread count. */
+#pragma omp parallel
+  {
+    real* h = (real*)malloc(sizeof(real) * (e1 + e2 + e1));
+    real* t = h + e1 + e2;
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < N; ++i) {
+      const int ia = o->order[i];
+      const real* xi = o->xs + 3 * i;
+      for (long k = o->lstart[i]; k < o->lstart[i + 1]; ++k) {
+        const int j = o->lj[k], ja = o->order[j];
+        const real* xj = o->xs + 3 * j;
+        real rsq = sqr(xi[0] - xj[0]) + sqr(xi[1] - xj[1]) + sqr(xi[2] - xj[2]);
+        if (!(rsq < cutsq)) continue;
+        real r = sqrt(rsq), u = r * r_rc;
+        int s = special_of(o, ia, ja);
+        const float *W1 = embw + eb * o->typ[ja], *b1 = W1 + e1, *W2 = b1 + e1, *b2 = W2 + (size_t)e1 * e2;
+        real cf = r - rc, cff = 1 - 1 / (1 + cf * cf);
+        for (int a = 0; a < e1; ++a) h[a] = tanh((real)W1[a] * u + (real)b1[a]);
+        for (int c = 0; c < e2; ++c) {
+          real z = (real)b2[c];
+          for (int a = 0; a < e1; ++a) z += h[a] * (real)W2[(size_t)a * e2 + c];
+          G[(size_t)ia * din + s * e2 + c] += scale * tanh(z) * cff;
+        }
       }
     }
-  }
-  double en = 0;
-  const size_t fb = fit_block(din, h1, h2);
-  for (int a = 0; a < N; ++a) {
-    double ea = fit_eval(fitw + fb * o->typ[a], din, h1, h2, G + (size_t)a * din, dG + (size_t)a * din);
-    if (e_atom) e_atom[a] = ea;
-    en += ea;
-  }
-  double w = 0;
-  for (int i = 0; i < N; ++i) {
-    const int ia = o->order[i];
-    const real* xi = o->xs + 3 * i;
-    real fx = 0, fy = 0, fz = 0;
-    for (long k = o->lstart[i]; k < o->lstart[i + 1]; ++k) {
-      const int j = o->lj[k], ja = o->order[j];
-      const real* xj = o->xs + 3 * j;
-      real dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
-      real rsq = sqr(dx) + sqr(dy) + sqr(dz);
-      if (!(rsq < cutsq)) continue;
-      real r = sqrt(rsq), u = r * r_rc;
-      int s = special_of(o, ia, ja);
-      real cf = r - rc, den = 1 + cf * cf, cff = 1 - 1 / den, dcff = 2 * cf / (den * den);
-      /* dE/dr_ij: G_i holds y_{t_j}(r) and G_j holds y_{t_i}(r), both in slot s */
-      real dEdr = emb_dedr(embw + eb * o->typ[ja], e1, e2, u, r_rc, cff, dcff, scale, dG + (size_t)ia * din + s * e2, h, t) +
-                  emb_dedr(embw + eb * o->typ[ia], e1, e2, u, r_rc, cff, dcff, scale, dG + (size_t)ja * din + s * e2, h, t);
-      real fpair = -dEdr / r;
-      fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
-      w += 0.5 * (double)(fpair * rsq);
+    const size_t fb = fit_block(din, h1, h2);
+#pragma omp for schedule(static)
+    for (int a = 0; a < N; ++a)
+      ea_all[a] = fit_eval(fitw + fb * o->typ[a], din, h1, h2, G + (size_t)a * din, dG + (size_t)a * din);
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < N; ++i) {
+      const int ia = o->order[i];
+      const real* xi = o->xs + 3 * i;
+      real fx = 0, fy = 0, fz = 0;
+      double wi = 0;
+      for (long k = o->lstart[i]; k < o->lstart[i + 1]; ++k) {
+        const int j = o->lj[k], ja = o->order[j];
+        const real* xj = o->xs + 3 * j;
+        real dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+        real rsq = sqr(dx) + sqr(dy) + sqr(dz);
+        if (!(rsq < cutsq)) continue;
+        real r = sqrt(rsq), u = r * r_rc;
+        int s = special_of(o, ia, ja);
+        real cf = r - rc, den = 1 + cf * cf, cff = 1 - 1 / den, dcff = 2 * cf / (den * den);
+        /* dE/dr_ij: G_i holds y_{t_j}(r) and G_j holds y_{t_i}(r), both in slot s */
+        real dEdr = emb_dedr(embw + eb * o->typ[ja], e1, e2, u, r_rc, cff, dcff, scale, dG + (size_t)ia * din + s * e2, h, t) +
+                    emb_dedr(embw + eb * o->typ[ia], e1, e2, u, r_rc, cff, dcff, scale, dG + (size_t)ja * din + s * e2, h, t);
+        real fpair = -dEdr / r;
+        fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
+        wi += 0.5 * (double)(fpair * rsq);
+      }
+      f_by_id[3 * ia] += fx; f_by_id[3 * ia + 1] += fy; f_by_id[3 * ia + 2] += fz;
+      w_all[i] = wi;
     }
-    f_by_id[3 * ia] += fx; f_by_id[3 * ia + 1] += fy; f_by_id[3 * ia + 2] += fz;
+    free(h);
   }
+  double en = 0, w = 0;
+  for (int a = 0; a < N; ++a) {
+    if (e_atom) e_atom[a] = ea_all[a];
+    en += ea_all[a];
+  }
+  for (int i = 0; i < N; ++i) w += w_all[i];
   if (G_out) for (size_t k = 0; k < (size_t)N * din; ++k) { G_out[k] = G[k]; dEdG_out[k] = dG[k]; }
   *e_net += en; *vir += w;
-  free(G); free(dG); free(h);
+  free(G); free(dG); free(ea_all); free(w_all);
   return 0;
 }
 
