@@ -178,6 +178,39 @@ def water_box(n_side: int, bl: float, seed: int, temperature: float = 300.0,
                   moltypes=[WATER], mol_type=np.zeros(nmol, np.int32), name=name)
 
 
+# Hydrogen peroxide H-O-O-H (atom order H1 O1 O2 H2): the smallest molecule with a dihedral, for
+# the bonded terms' parity. Types as water (O 0, H 1), so the water pair table applies. Bond types
+# 0 (O-H) and 1 (O-O), angle type 0 (H-O-O), dihedral type 0 (H-O-O-H).
+PEROXIDE = MoleculeType(n_atom=4, bonds=[(0, 0, 1), (1, 1, 2), (0, 2, 3)], angles=[(0, 0, 1, 2), (0, 1, 2, 3)],
+                        dihedrals=[(0, 0, 1, 2, 3)])
+PEROXIDE_Q = (-0.41, 0.41)
+PEROXIDE_R_OO, PEROXIDE_R_OH, PEROXIDE_THETA, PEROXIDE_PHI = 1.45, 0.97, 100.0, 115.0
+
+
+def peroxide_box(n_side: int, bl: float, seed: int, temperature: float = 300.0, name: str = "peroxide") -> System:
+    """H2O2 molecules on a cubic lattice of n_side^3 sites with seeded random orientations."""
+    rng = np.random.default_rng(seed)
+    nmol = n_side ** 3
+    ix, iy, iz = np.unravel_index(np.arange(nmol), (n_side,) * 3)
+    a = bl / n_side
+    centers = np.stack([ix, iy, iz], 1) * a - bl / 2 + a / 2
+    th, ph = math.radians(PEROXIDE_THETA), math.radians(PEROXIDE_PHI)
+    o1, o2 = np.array([-PEROXIDE_R_OO / 2, 0, 0]), np.array([PEROXIDE_R_OO / 2, 0, 0])
+    # H1 on O1 at angle theta from the O1->O2 axis in the xz plane; H2 on O2 rotated by the dihedral
+    h1 = o1 + PEROXIDE_R_OH * np.array([math.cos(th), 0.0, math.sin(th)])
+    h2 = o2 + PEROXIDE_R_OH * np.array([-math.cos(th), math.sin(th) * math.sin(ph), math.sin(th) * math.cos(ph)])
+    local = np.stack([h1, o1, o2, h2])
+    R = _random_rotations(rng, nmol)
+    x = (centers[:, None, :] + np.einsum("mij,aj->mai", R, local)).reshape(-1, 3)
+    x -= np.rint(x / bl) * bl
+    typ = np.tile(np.array([1, 0, 0, 1], np.int32), nmol)
+    mass = np.array(WATER_MASS, np.float32)[typ]
+    q = np.array(PEROXIDE_Q, np.float32)[typ]
+    v = maxwell_boltzmann(rng, mass, temperature)
+    return System(bl=float(bl), ntype=2, typ=typ, mass=mass, q=q, x=x.astype(np.float32), v=v,
+                  moltypes=[PEROXIDE], mol_type=np.zeros(nmol, np.int32), name=name)
+
+
 ATOM = MoleculeType(n_atom=1)
 
 

@@ -8,6 +8,7 @@ Coulomb, 2 A skin) or the two-species LJ+Coulomb mixture of the g(r)/S(q) worklo
 from __future__ import annotations
 
 import hashlib
+import math
 import os
 from typing import Dict
 
@@ -32,10 +33,72 @@ def water_case(n_side=6, bl=18.624, seed=1, temperature=300.0, nmol=None, jitter
     return s, (r, F, U)
 
 
+MIX_SIGMA, MIX_EPS = (3.0, 3.4), (0.15, 0.25)
+
+
+def mixture_table(eps_scale=1.0):
+    return S.lj_table(2, MIX_SIGMA, tuple(eps_scale * e for e in MIX_EPS), 10.0, 1000)
+
+
 def mixture_case(natom=2000, rho=0.035, seed=4):
     s = S.lj_mixture(natom, rho, 0.6, seed=seed)
-    r, F, U = S.lj_table(2, (3.0, 3.4), (0.15, 0.25), 10.0, 1000)
-    return s, (r, F, U)
+    return s, mixture_table()
+
+
+def water3000_case():
+    """The 3000-atom box of the plain workload: 1000 molecules on a 10^3 lattice in 31.04 A, seed 2."""
+    return water_case(n_side=10, bl=31.04, seed=2)
+
+
+def mixture30k_case():
+    """The 30,000-atom liquid of the g(r)/S(q) workload: 60/40 at 0.035 A^-3 (94.99 A box), seed 4."""
+    return mixture_case(natom=30000, rho=0.035, seed=4)
+
+
+PEROXIDE_BOND = ((0.97, 450.0), (1.45, 300.0))     # (b0, k) of bond types O-H, O-O
+PEROXIDE_ANGLE = (100.0, 50.0)                     # (theta0, kc) of H-O-O, harmonic in cos(theta)
+PEROXIDE_DIHEDRAL = (1.0, 1.5, -0.8, 0.3)          # c0 + c1 cos(phi) + c2 cos(2 phi) + c3 cos(3 phi)
+
+
+def peroxide_case(jitter=0.05):
+    """512 H2O2 molecules (2048 atoms) in a 30.4 A box, seed 9, atoms displaced by seeded N(0, jitter)."""
+    s = S.peroxide_box(8, 30.4, seed=9)
+    if jitter > 0:
+        rng = np.random.default_rng(1009)
+        s.x = (s.x + rng.normal(0, jitter, s.x.shape)).astype(np.float32)
+    return s, S.water_lj_table(10.0, 1000)
+
+
+def peroxide_bonded_cfg():
+    """The peroxide bonded terms as the reference harness's config lines (BOND/ANGLE/DIHEDRAL::setParam)."""
+    return {"bond": [f"{b0} {k}" for b0, k in PEROXIDE_BOND], "angle": [f"{PEROXIDE_ANGLE[0]} 0 0 {PEROXIDE_ANGLE[1]}"],
+            "dihedral": [" ".join(str(c) for c in PEROXIDE_DIHEDRAL)]}
+
+
+def bond_row(b0, ka=0.0, kb=0.0, kc=0.0):
+    """BOND::setParam's coefficient row (bond.cpp:27-33): (b0, 2 ka, kb, 2 kc) in float."""
+    f = np.float32
+    return np.array([f(b0), f(ka) * f(2), f(kb), f(kc) * f(2)], np.float32)
+
+
+def angle_row(theta0, ka=0.0, kb=0.0, kc=0.0):
+    """ANGLE::setParam's row (angle.cpp:26-32): (cos theta0, 2 ka, kb, 2 kc) in float."""
+    f = np.float32
+    return np.array([cos_theta0(theta0), f(ka) * f(2), f(kb), f(kc) * f(2)], np.float32)
+
+
+def dihedral_row(c0, c1, c2, c3):
+    """DIHEDRAL::setParam's row (dihedral.cpp:27-35): (c0 - c2, c1 - 3 c3, 4 c2, 12 c3) in float."""
+    f = np.float32
+    c0, c1, c2, c3 = f(c0), f(c1), f(c2), f(c3)
+    return np.array([c0 - c2, c1 - f(3) * c3, c2 * f(2) * f(2), c3 * f(4) * f(3)], np.float32)
+
+
+def peroxide_coefs():
+    """The peroxide terms as coefficient rows (the setParam transforms): (bond rows, angle rows,
+    dihedral rows)."""
+    return ([bond_row(b0, 0, 0, k) for b0, k in PEROXIDE_BOND], [angle_row(PEROXIDE_ANGLE[0], 0, 0, PEROXIDE_ANGLE[1])],
+            [dihedral_row(*PEROXIDE_DIHEDRAL)])
 
 
 def table_as_loaded(F, U):
@@ -74,18 +137,41 @@ def list_keys(rec: np.ndarray, natom: int):
     return counts, digests
 
 
+def block_digests(digests, block=1000):
+    """One 64-bit digest per block of `block` atoms over the per-atom list digests (a checksum of
+    checksums that keeps large fixtures small)."""
+    d = np.asarray(digests, np.uint64)
+    out = []
+    for k in range(0, len(d), block):
+        h = hashlib.blake2b(d[k:k + block].tobytes(), digest_size=8).digest()
+        out.append(np.frombuffer(h, np.uint64)[0])
+    return np.array(out, np.uint64)
+
+
+def x_digest(x):
+    return np.frombuffer(hashlib.blake2b(np.ascontiguousarray(x, np.float32).tobytes(), digest_size=8).digest(),
+                         np.uint64)[0]
+
+
 def rel_rms(a, b):
     a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
+def cos_theta0(theta0_deg: float) -> np.float32:
+    """cos(theta_0) as ANGLE::setParam computes it (angle.cpp:28): the argument theta*pi/180 in
+    float, the cosine correctly rounded to float (the library's nnpe_angle_coef gives the same
+    bits). Plain numpy, so that the reference's timing process loads no library of this project."""
+    f = np.float32
+    arg = f(f(theta0_deg) * f(3.141592653589793238462643383279502884)) / f(180)
+    return f(math.cos(float(arg)))
+
+
 def water_bonded_raw():
     """Raw (pre-setParam) bond/angle/dihedral coefficients of the water model, as the reference's
     NNP weight file stores them (pair_nnp.cpp:507-512): setParam() doubles entries 1 and 3."""
-    from nnpengine_b200 import engine as E
-    a = E.angle_coef(109.47, 0, 0, WATER_ANGLE_KC)
-    return (np.array([[1.0, 0, 0, WATER_BOND_K]], np.float32), np.array([[a[0], 0, 0, WATER_ANGLE_KC]], np.float32),
-            np.zeros((1, 4), np.float32))
+    return (np.array([[1.0, 0, 0, WATER_BOND_K]], np.float32),
+            np.array([[cos_theta0(109.47), 0, 0, WATER_ANGLE_KC]], np.float32), np.zeros((1, 4), np.float32))
 
 
 def write_nnp_inputs(m, d):

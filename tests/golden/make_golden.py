@@ -30,8 +30,9 @@ is run on the seeded cases of tests/cases.py; its outputs are stored compactly:
                  box (jittered, 60 bins to 6 A^-1) and of the 2000-atom mixture (40 bins to 3 A^-1):
                  the positions it used, mean |G| per bin, S(q) per type pair and G count per bin.
 
-Run:  python tests/golden/make_golden.py [name ...]   (needs /root/reference/src and
-`make -C oracle ref`; without names every fixture is written).
+Run:  python tests/golden/make_golden.py [name ...]   (needs the reference's sources, found by
+oracle.orc.refsrc(), and the harness that oracle.orc.build() compiles from them; without names
+every fixture is written).
 """
 from __future__ import annotations
 
@@ -185,7 +186,96 @@ def sqd2000(work):
     _sqd_fixture(work, "sqd2000", s, table, 40, 3.0)
 
 
-ALL = [water648, mixture2000, nnp_gauss648, rmdf2000, driver648, sqd648, sqd2000]
+def water3000(work):
+    """The 3000-atom water box of the plain workload (1000 molecules on a 10^3 lattice, 31.04 A box,
+    seed 2, 300 K Maxwell-Boltzmann): the reference's snapshot (list, images, forces, energies, g(r)
+    counts), 100 and 1000 NVE steps at 1 fs (energies every 10 steps, final x and v), and 5 ps at
+    1 fs under its Andersen thermostat at 300 K (the equilibrated state the network workload starts
+    from)."""
+    s, table = cases.water3000_case()
+    f = cases.write_inputs(s, table, work)
+    base = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10,
+            "velocity": f["vel"], **bonded_cfg()}
+    v0 = os.path.join(work, "v0.bin")     # the snapshot at rest: its positions are the input's exactly
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    snap = orc.run_ref_dump({**base, "velocity": v0, "mode": "snapshot"}, os.path.join(work, "snap"))
+    counts, digests = cases.list_keys(snap["fulllist"], s.natom)
+    md = {"mode": "md", "dt": 1, "log_interval": 10}
+    m100 = orc.run_ref_dump({**base, **md, "steps": 100}, os.path.join(work, "m100"))
+    m1000 = orc.run_ref_dump({**base, **md, "steps": 1000}, os.path.join(work, "m1000"))
+    eq = orc.run_ref_dump({**base, "mode": "md", "dt": 1, "log_interval": 1000, "steps": 5000, "temp": 300,
+                           "scale_interval": 10, "seed": 31}, os.path.join(work, "eq"))
+    out = dict(x=s.x, v=s.v, list_counts=counts, list_digests=digests, nghost=snap["info"]["nghost"],
+               force=snap["force"].reshape(-1, 3), erg_f32=snap["log_e"], vir_f32=snap["log_w"],
+               gr_counts=snap["gr_counts"].reshape(3, -1), gr_inner_counts=snap["gr_inner_counts"].reshape(3, -1),
+               md100_x=m100["x"].reshape(-1, 3), md100_v=m100["v"].reshape(-1, 3), md100_erg=m100["log_e"],
+               md100_ekin=m100["log_k"], md100_nbuild=m100["info"]["nbuild_last"],
+               md1000_erg=m1000["log_e"], md1000_ekin=m1000["log_k"], md1000_nbuild=m1000["info"]["nbuild_last"],
+               eq_x=eq["x"].reshape(-1, 3), eq_v=eq["v"].reshape(-1, 3), eq_ekin=eq["log_k"])
+    np.savez_compressed(os.path.join(HERE, "water3000.npz"), **out)
+    print("water3000:", s.natom, "atoms,", int(counts.sum()), "list entries,", snap["info"]["nghost"], "images;",
+          "1000-step nbuild", m1000["info"]["nbuild_last"], "; equilibrated T",
+          float(eq["log_k"][-1]) / s.natom * 2 / 3 / 0.0019872)
+
+
+def mixture30k(work):
+    """The 30,000-atom two-species liquid of the g(r)/S(q) workload (0.035 A^-3, seed 4): the
+    reference's g(r) counts to 15 A (cell-based) and to the list cutoff (list-based), its float
+    S(q), the list counts with block digests, the image count; and the RMDF target: the weighted
+    S(q) (RMDF's sq, what RMDF::dumpSQ writes) of the same liquid with every eps x1.1 after 500
+    steps at 1 fs under its Andersen thermostat at 300 K (seed 41)."""
+    from nnpengine_b200 import systems as S
+    s, table = cases.mixture30k_case()
+    f = cases.write_inputs(s, table, work)
+    v0 = os.path.join(work, "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    snap = orc.run_ref_dump({"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2,
+                             "gr_cutoff": 15, "nq": 512, "qmax": 20, "velocity": v0, "mode": "snapshot"},
+                            os.path.join(work, "snap"))
+    counts, digests = cases.list_keys(snap["fulllist"], s.natom)
+    # target: eps x1.1 table, g(r) step (cell-based) at md_step 0 and 500, RMDF of strength 0
+    r, F11, U11 = cases.mixture_table(eps_scale=1.1)
+    t11 = os.path.join(work, "table11.txt")
+    S.write_pair_table(t11, r, F11, U11)
+    q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, 2)
+    tpath = os.path.join(work, "sq_dummy.txt")
+    S.write_sq_target(tpath, q, sqex, wt, ff)
+    tgt = orc.run_ref_dump({"init": f["init"], "table": f"1000 {t11}", "cutoff": 10, "skin": 2, "gr_cutoff": 15,
+                            "nq": 512, "qmax": 20, "velocity": f["vel"], "mode": "md", "dt": 1, "steps": 500,
+                            "log_interval": 500, "temp": 300, "scale_interval": 10, "seed": 41,
+                            "gr_interval": "500 500", "rmdf": f"0 1 {tpath}"}, os.path.join(work, "tgt"))
+    out = dict(x_digest=cases.x_digest(s.x), natom=s.natom, list_counts=counts.astype(np.int32),
+               list_block_digests=cases.block_digests(digests), nghost=snap["info"]["nghost"],
+               gr_counts=snap["gr_counts"].reshape(3, -1), gr_inner_counts=snap["gr_inner_counts"].reshape(3, -1),
+               sq_f32=snap["sq"].reshape(3, -1), erg_f32=snap["log_e"],
+               target_sq=tgt["rmdf_sq"].astype(np.float32), target_q=q, target_wt=wt, target_ff=ff)
+    np.savez_compressed(os.path.join(HERE, "mixture30k.npz"), **out)
+    print("mixture30k:", s.natom, "atoms,", int(counts.sum()), "list entries; ordered pairs in the 15 A tally",
+          int(out["gr_counts"].sum()))
+
+
+def peroxide2048(work):
+    """512 H2O2 molecules (2048 atoms, 30.4 A box, seed 9, jittered 0.05 A) with bonds, angles and
+    the H-O-O-H dihedral: the reference's forces and energies with the water pair table, and its
+    bonded terms alone (no pair term), plus 20 NVE steps at 0.5 fs."""
+    s, table = cases.peroxide_case()
+    f = cases.write_inputs(s, table, work)
+    bcfg = cases.peroxide_bonded_cfg()
+    v0 = os.path.join(work, "v0.bin")
+    np.zeros((s.natom, 3), np.float32).tofile(v0)
+    base = {"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2, "gr_cutoff": 10, **bcfg}
+    snap = orc.run_ref_dump({**base, "velocity": v0, "mode": "snapshot"}, os.path.join(work, "snap"))
+    bond = orc.run_ref_dump({**base, "no_lj": "", "velocity": v0, "mode": "snapshot"}, os.path.join(work, "bond"))
+    md = orc.run_ref_dump({**base, "velocity": f["vel"], "mode": "md", "steps": 20, "dt": 0.5, "log_interval": 1},
+                          os.path.join(work, "md"))
+    out = dict(x=s.x, v=s.v, force=snap["force"].reshape(-1, 3), erg_f32=snap["log_e"],
+               f_bonded=bond["force"].reshape(-1, 3), erg_bonded=bond["log_e"],
+               md_x=md["x"].reshape(-1, 3), md_v=md["v"].reshape(-1, 3), md_erg=md["log_e"], md_ekin=md["log_k"])
+    np.savez_compressed(os.path.join(HERE, "peroxide2048.npz"), **out)
+    print("peroxide2048: bonded energy", float(bond["log_e"][0]), "total", float(snap["log_e"][0]))
+
+
+ALL = [water648, mixture2000, nnp_gauss648, rmdf2000, driver648, sqd648, sqd2000, water3000, mixture30k, peroxide2048]
 
 if __name__ == "__main__":
     names = sys.argv[1:]
