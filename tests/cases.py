@@ -189,11 +189,12 @@ def write_nnp_inputs(m, d):
 
 
 def write_run_input(d, mode, s, table=None, nnp_paths=None, temps=(0.0, 0.0), steps=(20, 5, 20, 5, 10),
-                    rmdf=None, nbin=1000, cutoffs=(10.0, 2.0, 10.0), nq=512, qmax=20.0, sqd=None):
+                    rmdf=None, nbin=1000, cutoffs=(10.0, 2.0, 10.0), nq=512, qmax=20.0, sqd=None, append=False):
     """The run input file of the reference's `classical` or `nnp_run` mode (run.cpp:25-50) for a
     case in directory d; rmdf = (strength, gamma, target file) or None (no target: n_sq 0, which
     the reference reads but cannot run, so its harness runs use one target of strength 0);
-    sqd = (q_max, nq) writes the direct S(q) of the final state, None skips it."""
+    sqd = (q_max, nq) writes the direct S(q) of the final state, None skips it; append: the output
+    lines ask for appending (running averages of the g(r), S(q), SQD and RMDF dumps)."""
     os.makedirs(d, exist_ok=True)
     init = os.path.join(d, "init.txt")
     S.write_init_file(init, s)
@@ -212,14 +213,39 @@ def write_run_input(d, mode, s, table=None, nnp_paths=None, temps=(0.0, 0.0), st
     lines.append(f"{temps[0]} {temps[1]}")
     lines.append(" ".join(str(v) for v in steps))
     out = {k: os.path.join(d, k + ".out") for k in ("xyz", "gr", "sq", "sqd", "sqx", "force")}
-    sqd_line = f"{out['sqd']} 0 {sqd[0]} {sqd[1]}" if sqd else "* 0 20 10"   # file append q_max nq
-    lines += [f"{out['xyz']} 0", f"{out['gr']} 0", f"{out['sq']} 0", sqd_line, f"{out['sqx']} 0"]
+    ap = int(bool(append))
+    sqd_line = f"{out['sqd']} {ap} {sqd[0]} {sqd[1]}" if sqd else "* 0 20 10"   # file append q_max nq
+    lines += [f"{out['xyz']} {ap}", f"{out['gr']} {ap}", f"{out['sq']} {ap}", sqd_line, f"{out['sqx']} {ap}"]
     if mode == "classical":
-        lines.append(f"{out['force']} 0")
+        lines.append(f"{out['force']} {ap}")
     path = os.path.join(d, "run.in")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
     return path, out
+
+
+def read_dump(path):
+    """An output file of the reference's formats as numbers: xyz frames (ENVIRON::dump,
+    environ.cpp:178-188) -> (frames [n][natom][3], types [natom], box half-lengths); the other
+    dumps (GR/SQ/SQD::dump, RMDF::dumpSQ, dumpForce) -> (accumulation count from the '# n'
+    header or 0, rows [m][cols])."""
+    with open(path) as f:
+        lines = [ln.split() for ln in f if ln.strip()]
+    if lines and lines[0][0].isdigit() and len(lines) > 1 and lines[1][:4] == ["x", "y", "z", "w"]:
+        frames, k = [], 0
+        while k < len(lines):
+            n = int(lines[k][0])
+            box = (float(lines[k + 1][4]), float(lines[k + 1][5]))
+            rows = lines[k + 2:k + 2 + n]
+            frames.append([[float(v) for v in r[1:4]] for r in rows])
+            types = [int(r[0][1:]) for r in rows]
+            k += 2 + n
+        return np.array(frames), np.array(types), box
+    num = 0
+    if lines and lines[0][0] == "#":
+        num = int(lines[0][1])
+        lines = lines[1:]
+    return num, np.array([[float(v) for v in r] for r in lines])
 
 
 def parse_log(text):

@@ -275,7 +275,46 @@ def peroxide2048(work):
     print("peroxide2048: bonded energy", float(bond["log_e"][0]), "total", float(snap["log_e"][0]))
 
 
-ALL = [water648, mixture2000, nnp_gauss648, rmdf2000, driver648, sqd648, sqd2000, water3000, mixture30k, peroxide2048]
+def dumps648(work):
+    """Content of the reference executable's output files (oracle/_ref/nnp.exe, run.cpp + main.cpp
+    unmodified) in both modes for the 648-atom water box: total_steps 0 at 0 K, so that every file
+    holds the starting configuration's xyz, g(r), S(q), RMDF S(q) and (classical) the RMDF-updated
+    force table, none of which depends on its unseeded generator; run twice with the append flags
+    on, so that the files hold the running averages (count 2) and two xyz frames. (The executable's
+    direct S(q) line, run.cpp:420-432, ends in a segmentation fault on these inputs whatever the run
+    length; the direct S(q) file is pinned through the harness in sqd648 instead.)"""
+    import subprocess
+    from nnpengine_b200 import nnp_model as NM
+    out = {}
+    for mode in ("classical", "nnp_run"):
+        d = os.path.join(work, mode)
+        os.makedirs(d, exist_ok=True)
+        s, table = cases.water_case()
+        tpath, _ = rmdf_target(d)
+        kw = dict(rmdf=(RMDF_STRENGTH, RMDF_GAMMA, tpath), steps=(0, 1, 1000, 1, 1), append=True)
+        if mode == "classical":
+            path, files = cases.write_run_input(d, mode, s, table, **kw)
+        else:
+            paths = cases.write_nnp_inputs(NM.gauss_model(), d)
+            path, files = cases.write_run_input(d, mode, s, nnp_paths=paths, nbin=750, cutoffs=(6.0, 2.0, 6.0), **kw)
+        for _ in range(2):
+            subprocess.run([os.path.join(orc.REF_DIR, "nnp.exe"), mode, path], capture_output=True, text=True,
+                           timeout=600, check=True)
+        frames, types, box = cases.read_dump(files["xyz"])
+        out[f"{mode}_xyz"] = frames
+        out[f"{mode}_xyz_types"] = types
+        out[f"{mode}_xyz_box"] = np.array(box)
+        for k in ("gr", "sq", "sqd", "sqx", "force"):
+            if os.path.exists(files[k]):
+                num, rows = cases.read_dump(files[k])
+                out[f"{mode}_{k}_num"] = num
+                out[f"{mode}_{k}"] = rows
+        print(f"dumps648 {mode}:", {k: out[f'{mode}_{k}'].shape for k in ("gr", "sq", "sqd", "sqx") if f'{mode}_{k}' in out})
+    np.savez_compressed(os.path.join(HERE, "dumps648.npz"), **out)
+
+
+ALL = [water648, mixture2000, nnp_gauss648, rmdf2000, driver648, sqd648, sqd2000, water3000, mixture30k, peroxide2048,
+       dumps648]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

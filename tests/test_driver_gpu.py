@@ -95,3 +95,45 @@ def test_reference_style_loop_through_adapter_matches_step_loop(tmp_path):
     e.sqd_dump(str(tmp_path / "sqd_engine.txt"))
     assert open(sqd_out).read() == open(str(tmp_path / "sqd_engine.txt")).read()
     e.close()
+
+
+@pytest.mark.parametrize("mode", ["classical", "nnp_run"])
+def test_driver_output_files_match_reference_values(tmp_path, mode):
+    """The output files' contents, value by value, against the reference executable's on the same
+    run file: total_steps 0 at 0 K (nothing depends on the reference's unseeded generator), run
+    twice with the append flags on, so the g(r), S(q) and RMDF S(q) files hold running averages of
+    count 2 and the xyz file two frames (ENVIRON::dump environ.cpp:178-188, GR::dump
+    grsq.cpp:221-256, SQ::dump grsq.cpp:324-360, RMDF::dumpSQ grsq.cpp:1380-1416, dumpForce
+    pair.cpp:421-437)."""
+    g = np.load(os.path.join(cases.GOLDEN, "dumps648.npz"))
+    d = str(tmp_path / mode)
+    os.makedirs(d, exist_ok=True)
+    s, table = cases.water_case()
+    q, sqex, wt, ff = S.synthetic_sq_target(512, 20.0, 2, seed=7)
+    tpath = os.path.join(d, "sq_target.txt")
+    S.write_sq_target(tpath, q, sqex, wt, ff)
+    kw = dict(rmdf=(STRENGTH, GAMMA, tpath), steps=(0, 1, 1000, 1, 1), append=True)
+    if mode == "classical":
+        path, files = cases.write_run_input(d, mode, s, table, **kw)
+    else:
+        paths = cases.write_nnp_inputs(NM.gauss_model(), d)
+        path, files = cases.write_run_input(d, mode, s, nnp_paths=paths, nbin=750, cutoffs=(6.0, 2.0, 6.0), **kw)
+    for _ in range(2):
+        r = subprocess.run([build.DRIVER, mode, path, "--seed", "5", "--fp32-state"], capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+    frames, types, box = cases.read_dump(files["xyz"])
+    np.testing.assert_array_equal(frames, g[f"{mode}_xyz"])          # FP32 positions, printed %.15e
+    np.testing.assert_array_equal(types, g[f"{mode}_xyz_types"])
+    np.testing.assert_allclose(box, g[f"{mode}_xyz_box"], rtol=1e-7)
+    for k, rtol, atol_frac in (("gr", 2e-6, 2e-6), ("sq", 0, 1e-3), ("sqx", 0, 1e-3), ("force", 1e-4, 1e-4)):
+        if f"{mode}_{k}" not in g:
+            assert not os.path.exists(files[k])
+            continue
+        num, rows = cases.read_dump(files[k])
+        ref = g[f"{mode}_{k}"]
+        assert num == int(g[f"{mode}_{k}_num"])
+        assert rows.shape == ref.shape, (k, rows.shape, ref.shape)
+        np.testing.assert_allclose(rows[:, 0], ref[:, 0], rtol=1e-6)        # r or q grid
+        vals, rvals = rows[:, 1:], ref[:, 1:]
+        np.testing.assert_allclose(vals, rvals, rtol=rtol, atol=atol_frac * np.abs(rvals).max(), err_msg=k)
