@@ -94,6 +94,14 @@ int nnpe_init_velocities(nnpe_ctx* ctx, double temperature, double frac, uint64_
 /* neigh_cap: per-atom list capacity (NEIGH_SZ, run.h:2). nnp_cutoff > 0 adds the short
  * descriptor cutoff of a network term sharing the same list. */
 int nnpe_setup(nnpe_ctx* ctx, double pair_cutoff, double skin, double gr_cutoff, int neigh_cap);
+/* BL_MANAGER::setBL (run.cpp:688-712) with ENVIRON::set_bl (environ.h:105): a new cubic box length
+ * for a set-up context. The grid keeps its cell length (half of cutoff + skin) and is re-derived
+ * for the box, with its stencils and ghost limit; arrays that depend on the grid or on the image
+ * count are reallocated. Positions are kept (they are in the caller's new box after
+ * nnpe_set_positions or nnpe_force_step); the next evaluation rebuilds the list; the step counter
+ * and the list-build count restart, as after nnpe_setup. A direct S(q) set-up holds the box it
+ * was made for: call nnpe_sqd_setup again after a change. */
+int nnpe_set_box(nnpe_ctx* ctx, double bl);
 
 /* ---- LJTableCoulDSF (pair.h:30-54) ---------------------------------------------------- */
 /* Tables [npair][nbin+1] of F(r)/r and U(r) at r=(i+.5)dr, dr=cutoff/nbin, last column 0

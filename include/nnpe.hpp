@@ -109,6 +109,20 @@ class LOCAL {
 };
 
 /* neighlist.h:6-47 */
+/* run.h:9-21, run.cpp:688-729: a new box length per configuration (variable-box training). setBL
+ * re-derives the grid, stencils and ghost limit on the device (nnpe_set_box); the stencil it
+ * returns in the reference lives on the device here, so the returned pointer is null, as
+ * NEIGHLIST::build_bin_list's. */
+class BL_MANAGER {
+ public:
+  BL_MANAGER(numtype /*grid_length*/, numtype /*ghost_cutoff*/, numtype /*list_cutoff*/) {}
+  int** setBL(numtype bl) {
+    check(nnpe_set_box(ENVIRON::ctx, bl), "BL_MANAGER::setBL", ENVIRON::ctx);
+    ENVIRON::bl = bl;
+    return nullptr;
+  }
+};
+
 class NEIGHLIST {
  public:
   int thread_id, nbuild = 0;

@@ -41,6 +41,7 @@ _SIGS = {
     "nnpe_set_positions": (C.c_int, [_vp, _f32p]),
     "nnpe_set_velocities": (C.c_int, [_vp, _f32p]),
     "nnpe_setup": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_int]),
+    "nnpe_set_box": (C.c_int, [_vp, C.c_double]),
     "nnpe_pair_set_table": (C.c_int, [_vp, C.c_int, _f32p, _f32p]),
     "nnpe_pair_load_table": (C.c_int, [_vp, C.c_int, C.c_char_p]),
     "nnpe_pair_get_table": (C.c_int, [_vp, _f32p, _f32p]),

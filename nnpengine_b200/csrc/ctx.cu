@@ -413,6 +413,21 @@ int nnpe_setup(nnpe_ctx* c, double pair_cutoff, double skin, double gr_cutoff, i
   return NNPE_OK;
 }
 
+// A new box length for a set-up context: ENVIRON::set_bl plus BL_MANAGER::setBL (run.cpp:688-712),
+// i.e. the box constants in float, the grid re-derived with the same cell length, the ghost limit
+// and the stencils for the new grid; the device arrays that depend on the grid or on the number of
+// images are reallocated for it. The positions stay as they are (set new ones with
+// nnpe_set_positions or pass them to nnpe_force_step); the next force evaluation rebuilds the list.
+int nnpe_set_box(nnpe_ctx* c, double bl) {
+  if (!c || !c->have_setup || !(bl > 0)) return nnpe_fail(c, NNPE_EARG, "nnpe_set_box: not set up, or box length <= 0");
+  if (int rc = refuse_if_poisoned(c)) return rc;
+  const float blf = (float)bl;
+  c->bl = bl;
+  c->grid.bl = blf; c->grid.r_bl = 1.0f / blf; c->grid.h_bl = blf * .5F; c->grid.m_bl = -blf;
+  c->force_step_init = false;
+  return nnpe_setup(c, c->pair_cutoff, c->skin, c->gr_cutoff, c->cap);
+}
+
 // ---------------------------------------------------------------------------------------------
 // pair table
 // ---------------------------------------------------------------------------------------------

@@ -105,6 +105,10 @@ class Engine:
         self._ok(self.lib.nnpe_setup(self.h, pair_cutoff, skin, gr_cutoff or pair_cutoff, neigh_cap))
 
     # ---- LJTableCoulDSF --------------------------------------------------------------------
+    def set_box(self, bl: float):
+        """BL_MANAGER::setBL: a new cubic box length (grid, stencils and ghost limit follow)."""
+        self._ok(self.lib.nnpe_set_box(self.h, bl))
+
     def set_pair_table(self, F, U):
         """F, U: [npair, nbin] or [npair, nbin+1] (the extra zero column is added)."""
         F = np.asarray(F, np.float32); U = np.asarray(U, np.float32)

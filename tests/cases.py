@@ -40,6 +40,12 @@ def mixture_table(eps_scale=1.0):
     return S.lj_table(2, MIX_SIGMA, tuple(eps_scale * e for e in MIX_EPS), 10.0, 1000)
 
 
+def rescaled(s, bl):
+    """System s with box length bl and positions scaled by bl / s.bl (float32)."""
+    import dataclasses
+    return dataclasses.replace(s, bl=float(bl), x=(np.asarray(s.x, np.float64) * (bl / s.bl)).astype(np.float32))
+
+
 def mixture_case(natom=2000, rho=0.035, seed=4):
     s = S.lj_mixture(natom, rho, 0.6, seed=seed)
     return s, mixture_table()

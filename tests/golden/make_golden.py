@@ -313,8 +313,31 @@ def dumps648(work):
     np.savez_compressed(os.path.join(HERE, "dumps648.npz"), **out)
 
 
+def box648(work):
+    """The 648-atom water box rescaled to other box lengths (positions times bl / 18.624, a smaller
+    box and a larger one whose grid has more cells): the reference's snapshot at each, for the
+    variable-box path (BL_MANAGER::setBL, run.cpp:688-712)."""
+    s, table = cases.water_case()
+    out = {}
+    for tag, bl in (("small", 18.0), ("large", 25.0)):
+        sb = cases.rescaled(s, bl)
+        d = os.path.join(work, tag)
+        f = cases.write_inputs(sb, table, d)
+        v0 = os.path.join(d, "v0.bin")
+        np.zeros((sb.natom, 3), np.float32).tofile(v0)
+        snap = orc.run_ref_dump({"init": f["init"], "table": f"1000 {f['table']}", "cutoff": 10, "skin": 2,
+                                 "gr_cutoff": 10, **bonded_cfg(), "velocity": v0, "mode": "snapshot"},
+                                os.path.join(d, "snap"))
+        counts, digests = cases.list_keys(snap["fulllist"], sb.natom)
+        out.update({f"{tag}_bl": np.float64(bl), f"{tag}_x": sb.x, f"{tag}_list_counts": counts,
+                    f"{tag}_list_digests": digests, f"{tag}_nghost": snap["info"]["nghost"],
+                    f"{tag}_force": snap["force"].reshape(-1, 3)})
+        print(f"box648 {tag}: bl {bl}, {int(counts.sum())} list entries, {snap['info']['nghost']} images")
+    np.savez_compressed(os.path.join(HERE, "box648.npz"), **out)
+
+
 ALL = [water648, mixture2000, nnp_gauss648, rmdf2000, driver648, sqd648, sqd2000, water3000, mixture30k, peroxide2048,
-       dumps648]
+       dumps648, box648]
 
 if __name__ == "__main__":
     names = sys.argv[1:]

@@ -75,3 +75,22 @@ def test_peroxide_dihedral_forces():
     o.rebuild(s.x, 10, 2, 12)
     fnd, _, _ = o.bonded(np.array(b), np.array(a), np.zeros((1, 4), np.float32))
     assert cases.rel_rms(fnd, g["f_bonded"]) > 1e-3
+
+
+def test_rescaled_boxes_list_and_forces():
+    """The restatement at the box lengths of the variable-box fixture: pair set bit-exact, forces."""
+    g = golden("box648.npz")
+    s, table = cases.water_case()
+    F, U = cases.table_as_loaded(table[1], table[2])
+    for tag in ("small", "large"):
+        sb = cases.rescaled(s, float(g[f"{tag}_bl"]))
+        np.testing.assert_array_equal(sb.x, g[f"{tag}_x"])
+        o = orc.Restated(sb, "f32")
+        assert o.rebuild(sb.x, 10, 2, 12) == 0
+        assert o.nghost == int(g[f"{tag}_nghost"])
+        counts, digests = cases.list_keys(o.list_records(), sb.natom)
+        np.testing.assert_array_equal(counts, g[f"{tag}_list_counts"])
+        np.testing.assert_array_equal(digests, g[f"{tag}_list_digests"])
+        f, _, _ = o.pair_forces(F, U, 10.0)
+        fb, _, _ = o.bonded(*water_rows())
+        assert cases.rel_rms(f + fb, g[f"{tag}_force"]) < 1e-5
