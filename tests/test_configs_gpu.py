@@ -259,7 +259,10 @@ def test_peroxide_dihedral_parity():
 def test_network_forces_are_gradient_of_gpu_energy():
     """Central differences of the GPU's own network energy (FP32 network, per-atom energies summed
     in FP64) against the GPU's forces, on 8 atoms x 3 directions of the jittered 648-atom water box:
-    ties the hand-written backward to the forward without the oracle."""
+    ties the hand-written backward to the forward without the oracle. The FP32 energy carries about
+    2e-6 kcal/mol of rounding noise from evaluation to evaluation, so the step is 0.02 A, where a
+    central difference resolves the forces (RMS 0.04 kcal/mol/A) to about 2e-3 of their RMS; a wrong
+    term in the backward would be off by order one."""
     s, _ = cases.water_case(jitter=0.05)
     m = NM.embed_model()
     e = Engine(0)
@@ -275,7 +278,7 @@ def test_network_forces_are_gradient_of_gpu_energy():
     f0 = e.forces().astype(np.float64)
     frms = np.sqrt((f0 ** 2).sum(1).mean())
     rng = np.random.default_rng(3)
-    h = np.float32(4e-3)
+    h = np.float32(2e-2)
     worst = 0.0
     for a in rng.choice(s.natom, 8, replace=False):
         for dim in range(3):
@@ -290,5 +293,5 @@ def test_network_forces_are_gradient_of_gpu_energy():
             fd = -(ep[0][0] - ep[1][0]) / (float(ep[0][1]) - float(ep[1][1]))
             worst = max(worst, abs(fd - f0[a, dim]) / frms)
     print(f"finite difference vs forces: worst {worst:.2e} of the force RMS {frms:.3f}")
-    assert worst < 2e-3
+    assert worst < 5e-3
     e.close()
