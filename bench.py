@@ -317,7 +317,7 @@ def serve_bench(args, wl):
     from nnpengine_b200 import systems as S
     from nnpengine_b200.serve import Server
     nreq = args.serve_requests
-    trace = S.serving_trace(nreq, seed=3)
+    trace = S.serving_trace(nreq, seed=3, rate=args.serve_rate)
     for t in trace:
         t["nsteps"] = max(20, int(round(t["nsteps"] * args.serve_scale)))
     boxes = [S.water_request_box(t["natom"], t["density"], t["seed"], t["temperature"]) for t in trace]
@@ -549,6 +549,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-scale", type=float, default=1.0, help="multiply every request's step count")
     ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the request stream [1/s]")
     ap.add_argument("--serve-timeout", type=float, default=900.0)
     ap.add_argument("--drift-ps", type=float, default=-1.0,
                     help="after the timed steps, NVE for this many ps (-1: 10 ps for the network workloads)")
@@ -628,6 +629,7 @@ def main():
             "steps": res["total_steps"], "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded request stream)",
             "config": {"workload": args.workload, "description": wl["desc"], "serve_scale": args.serve_scale,
+                       "arrival_rate_per_s": args.serve_rate,
                        "slots": args.serve_slots, "autotune": not args.no_autotune, "timing": "host clock: first arrival to last completion"},
             "latency_s": {"p50": res["p50_s"], "p99": res["p99_s"], "mean": res["mean_s"]},
             "serving": res, "cpu_baseline": cpu, "clocks": res["clocks"],

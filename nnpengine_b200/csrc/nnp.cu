@@ -124,7 +124,7 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   if ((kind != 0 && kind != 1) || !(cutoff > 0) || h1 <= 0 || h2 <= 0 || h1 > 256 || h2 > 256 || !fitw)
     return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: bad network shape");
   if ((float)cutoff > c->pair_cutoff + c->skin) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: network cutoff beyond the list");
-  if (kind == 1 && (e1 != 32 || e2 <= 0 || e2 > 64 || !embw)) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: embedding must be 1->32->e2 (e2<=64)");
+  if (kind == 1 && (e1 != 32 || e2 != 64 || !embw)) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: embedding must be 1->32->64");
   if (kind == 0 && (nbin <= 0 || !coef_p || !coef_w || !coef_d || !coef_r)) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_set: tables need coefficients");
   cudaSetDevice(c->device);
   nnp_free(c);
@@ -169,8 +169,9 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   NNPE_CUDA(c, cudaMemcpy(m->d_soff_dev, m->soff.data(), sizeof(int) * m->soff.size(), cudaMemcpyHostToDevice));
   if (kind == 1) {
     const size_t eb = (size_t)32 + 32 + 32 * (size_t)e2 + e2;
-    const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * 32 * (e2 + 1)) + sizeof(int) * kEmbWarpsHost * 32);
-    const int smem_force = (int)(sizeof(float) * eb * c->ntype);
+    const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * 32 * (e2 + 1) + 32 * kEmbWarpsHost * 32) +
+                                sizeof(int) * kEmbWarpsHost * 32);
+    const int smem_force = (int)(sizeof(float) * (eb * c->ntype + 32 * kEmbWarpsHost * 32));
     if (int r2 = nnp_set_smem_attrs(c, smem_desc, smem_force)) return r2;
   }
   c->graph_valid = false;
@@ -347,17 +348,45 @@ __global__ void __launch_bounds__(128) k_gauss_force(NnpArgs a) {
   }
 }
 
+// First layer h = tanh(W1 u + b1) of the embedding net wt (W1[32] b1[32] W2[32][64] b2[64]) into this
+// thread's shared-memory slots hs[q * h_stride] (the e1 = 32, e2 = 64 network of this path).
+__device__ __forceinline__ void emb_layer1(const float* wt, float u, float* hs, int h_stride) {
+#pragma unroll
+  for (int q = 0; q < 32; ++q) hs[q * h_stride] = tanhf(wt[q] * u + wt[32 + q]);
+}
+// Channels [c0, c0 + 32) of the second layer's pre-activations z = b2 + W2^T h, h from the slots:
+// 32 sums in registers, each W2 row chunk read as 16-byte broadcasts (all lanes read the same row).
+__device__ __forceinline__ void emb_layer2_half(const float* wt, const float* hs, int h_stride, int c0, float* z) {
+  const float4* b2 = reinterpret_cast<const float4*>(wt + 64 + 32 * 64 + c0);
+#pragma unroll
+  for (int c4 = 0; c4 < 8; ++c4) {
+    const float4 b = b2[c4];
+    z[4 * c4] = b.x; z[4 * c4 + 1] = b.y; z[4 * c4 + 2] = b.z; z[4 * c4 + 3] = b.w;
+  }
+#pragma unroll 8
+  for (int q = 0; q < 32; ++q) {
+    const float4* row = reinterpret_cast<const float4*>(wt + 64 + q * 64 + c0);
+    const float hq = hs[q * h_stride];
+#pragma unroll
+    for (int c4 = 0; c4 < 8; ++c4) {
+      const float4 w4 = row[c4];
+      z[4 * c4] += hq * w4.x; z[4 * c4 + 1] += hq * w4.y; z[4 * c4 + 2] += hq * w4.z; z[4 * c4 + 3] += hq * w4.w;
+    }
+  }
+}
+
 // ---- embedding descriptor (FP32): one warp per atom, lanes over pairs; each lane evaluates its
 // pair's e1->e2 embedding with the weights of the neighbour's species from shared memory, then
 // the warp reduces channel sums per special class through shared memory (deterministic order).
 constexpr int kEmbWarps = 4;
-__global__ void __launch_bounds__(kEmbWarps * 32) k_emb_desc_f32(NnpArgs a) {
+__global__ void __launch_bounds__(kEmbWarps * 32, 3) k_emb_desc_f32(NnpArgs a) {
   extern __shared__ float sm[];
   const int E1 = 32, E2 = a.e2;
   const size_t eb = (size_t)E1 + E1 + (size_t)E1 * E2 + E2;
   float* W = sm;                                   // [ntype][eb]
   float* Y = sm + eb * a.ntype;                    // [warps][32][E2+1]
   int* S = (int*)(Y + kEmbWarps * 32 * (E2 + 1));  // [warps][32]
+  float* Hs = (float*)(S + kEmbWarps * 32);        // [32][threads]: first-layer values of each thread's pair
   for (int k = threadIdx.x; k < (int)(eb * a.ntype); k += blockDim.x) W[k] = a.embw[k];
   __syncthreads();
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
@@ -381,16 +410,14 @@ __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_desc_f32(NnpArgs a) {
       const float u = r * r_rc, cf = r - a.rc, cff = a.scale * (1.f - 1.f / (1.f + cf * cf));
       s = ent >> 30;
       const float* w = W + eb * ((ent >> 27) & 7);
-      float h[32];
+      float* hs = Hs + threadIdx.x;
+      emb_layer1(w, u, hs, blockDim.x);
 #pragma unroll
-      for (int q = 0; q < 32; ++q) h[q] = tanhf(w[q] * u + w[32 + q]);
-      const float* W2 = w + 64;
-      const float* b2 = W2 + 32 * E2;
-      for (int cc = 0; cc < E2; ++cc) {
-        float z = b2[cc];
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        float z[32];
+        emb_layer2_half(w, hs, blockDim.x, c0, z);
 #pragma unroll
-        for (int q = 0; q < 32; ++q) z += h[q] * W2[q * E2 + cc];
-        Yw[lane * (E2 + 1) + cc] = tanhf(z) * cff;
+        for (int cc = 0; cc < 32; ++cc) Yw[lane * (E2 + 1) + c0 + cc] = tanhf(z[cc]) * cff;
       }
     } else {
       for (int cc = 0; cc < E2; ++cc) Yw[lane * (E2 + 1) + cc] = 0.f;
@@ -425,36 +452,65 @@ __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_desc_f32(NnpArgs a) {
 // ---- embedding force (FP32): recompute the pair's embedding, back-propagate
 // a_c = scale*(dE/dG_i + dE/dG_j)[s*e2+c] through it to dE/dr, fpair = -dE/dr / r.
 // d/dr of sum_c scale * (ga + gb)[c] * y_c(r) * cff(r) for the embedding net wt (W1 b1 W2 b2).
+// Register-blocked: the 64 second-layer values of a pair live in registers and every W2 row is read
+// as 16-byte broadcasts (all lanes of a warp read the same row), four FMAs per shared-memory load.
+// hs: this thread's slots for the 32 first-layer values in shared memory (stride h_stride), kept
+// there across the backward so that the 64 channel values and the row sums fit in registers.
 __device__ __forceinline__ float emb_dedr(const float* wt, int E2, float u, float r_rc, float cff, float dcff,
-                                          float scale, const float* ga, const float* gb) {
-  float h[32], t[32];
+                                          float scale, const float* ga, const float* gb, float* hs, int h_stride) {
+  emb_layer1(wt, u, hs, h_stride);
+  float t[32];
 #pragma unroll
-  for (int q = 0; q < 32; ++q) { h[q] = tanhf(wt[q] * u + wt[32 + q]); t[q] = 0.f; }
-  const float* W2 = wt + 64;
-  const float* b2 = W2 + 32 * E2;
+  for (int q = 0; q < 32; ++q) t[q] = 0.f;
   float dEdr = 0.f;
-  for (int cc = 0; cc < E2; ++cc) {
-    float z = b2[cc];
 #pragma unroll
-    for (int q = 0; q < 32; ++q) z += h[q] * W2[q * E2 + cc];
-    const float y = tanhf(z);
-    const float ac = scale * (gb ? ga[cc] + gb[cc] : ga[cc]);
-    dEdr += ac * y * dcff;
-    const float g = ac * cff * (1.f - y * y);
+  for (int c0 = 0; c0 < 64; c0 += 32) {   // 32 channels at a time: their z, then their share of t
+    float g[32];
+    emb_layer2_half(wt, hs, h_stride, c0, g);
 #pragma unroll
-    for (int q = 0; q < 32; ++q) t[q] += g * W2[q * E2 + cc];
+    for (int cc = 0; cc < 32; cc += 4) {
+      float4 a4 = *reinterpret_cast<const float4*>(ga + c0 + cc);
+      if (gb) {
+        const float4 b4 = *reinterpret_cast<const float4*>(gb + c0 + cc);
+        a4.x += b4.x; a4.y += b4.y; a4.z += b4.z; a4.w += b4.w;
+      }
+      const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float y = tanhf(g[cc + e]);
+        const float ac = scale * av[e];
+        dEdr += ac * y * dcff;
+        g[cc + e] = ac * cff * (1.f - y * y);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      const float4* row = reinterpret_cast<const float4*>(wt + 64 + q * 64 + c0);
+      float t0 = 0.f, t1 = 0.f;
+#pragma unroll
+      for (int c4 = 0; c4 < 8; c4 += 2) {
+        const float4 w4 = row[c4], w5 = row[c4 + 1];
+        t0 += g[4 * c4] * w4.x + g[4 * c4 + 1] * w4.y + g[4 * c4 + 2] * w4.z + g[4 * c4 + 3] * w4.w;
+        t1 += g[4 * c4 + 4] * w5.x + g[4 * c4 + 5] * w5.y + g[4 * c4 + 6] * w5.z + g[4 * c4 + 7] * w5.w;
+      }
+      t[q] += t0 + t1;
+    }
   }
 #pragma unroll
-  for (int q = 0; q < 32; ++q) dEdr += t[q] * (1.f - h[q] * h[q]) * wt[q] * r_rc;
+  for (int q = 0; q < 32; ++q) {
+    const float hq = hs[q * h_stride];
+    dEdr += t[q] * (1.f - hq * hq) * wt[q] * r_rc;
+  }
   return dEdr;
 }
 
 template <bool EV>
-__global__ void __launch_bounds__(kEmbWarps * 32) k_emb_force_f32(NnpArgs a) {
+__global__ void __launch_bounds__(kEmbWarps * 32, 3) k_emb_force_f32(NnpArgs a) {
   extern __shared__ float sm[];
   const int E1 = 32, E2 = a.e2;
   const size_t eb = (size_t)E1 + E1 + (size_t)E1 * E2 + E2;
   float* W = sm;
+  float* Hs = sm + eb * a.ntype;   // [32][threads]: first-layer values of each thread's pair
   for (int k = threadIdx.x; k < (int)(eb * a.ntype); k += blockDim.x) W[k] = a.embw[k];
   __syncthreads();
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
@@ -480,14 +536,13 @@ __global__ void __launch_bounds__(kEmbWarps * 32) k_emb_force_f32(NnpArgs a) {
     const int s = ent >> 30, tj = (ent >> 27) & 7;
     const float* dGj = a.dG + (size_t)owner_of(j, a.N, a.gowner) * 4 * E2 + s * E2;
     const float* dGis = dGi + s * E2;
-    // the pair sits in G_i through the net of t_j and in G_j through the net of t_i
-    float dEdr;
-    if (tj == ti) {
-      dEdr = emb_dedr(W + eb * tj, E2, u, r_rc, cff, dcff, a.scale, dGis, dGj);
-    } else {
-      dEdr = emb_dedr(W + eb * tj, E2, u, r_rc, cff, dcff, a.scale, dGis, nullptr) +
-             emb_dedr(W + eb * ti, E2, u, r_rc, cff, dcff, a.scale, dGj, nullptr);
-    }
+    // the pair sits in G_i through the net of t_j and in G_j through the net of t_i (one net
+    // evaluation with the two dE/dG rows added when the species agree)
+    float dEdr = 0.f;
+    const int ndir = tj == ti ? 1 : 2;
+    for (int dir = 0; dir < ndir; ++dir)
+      dEdr += emb_dedr(W + eb * (dir ? ti : tj), E2, u, r_rc, cff, dcff, a.scale, dir ? dGj : dGis,
+                       ndir == 1 ? dGj : nullptr, Hs + threadIdx.x, blockDim.x);
     const float fpair = -dEdr / r;
     fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
     if (EV) w += 0.5 * (double)(fpair * rsq);
@@ -677,7 +732,8 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
     k_gauss_desc<<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
   } else {
     const size_t eb = (size_t)32 + 32 + 32 * (size_t)m->e2 + m->e2;
-    const size_t smem = sizeof(float) * (eb * c->ntype + kEmbWarps * 32 * (m->e2 + 1)) + sizeof(int) * kEmbWarps * 32;
+    const size_t smem = sizeof(float) * (eb * c->ntype + kEmbWarps * 32 * (m->e2 + 1) + 32 * kEmbWarps * 32) +
+                        sizeof(int) * kEmbWarps * 32;
     k_emb_desc_f32<<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
   }
   if (int rc = fit_f32_enqueue(c)) return rc;
@@ -686,7 +742,7 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
     else k_gauss_force<false><<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
   } else {
     const size_t eb = (size_t)32 + 32 + 32 * (size_t)m->e2 + m->e2;
-    const size_t smem = sizeof(float) * eb * c->ntype;
+    const size_t smem = sizeof(float) * (eb * c->ntype + 32 * kEmbWarps * 32);
     if (ev) k_emb_force_f32<true><<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
     else k_emb_force_f32<false><<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
   }

@@ -15,7 +15,8 @@
 //  k_tc_fit     128 atoms of one species per tile (G rows fetched by cp.async straight into the
 //               K-major A tile): G -> h1 -> h2 -> E forward and the hand-written
 //               backward dE/dG = ((A3 (1-h2^2)) A2^T (1-h1^2)) A1^T as four MMA chains (N = 128, 128,
-//               128, 256); activations stay in shared memory, weights stream through two buffers.
+//               128, 256); activations stay in shared memory; the backward reads the forward's
+//               weight images as MN-major (transposed) tiles.
 //  k_tc_force2  second layer and its r-derivative per directed pair (two MMAs), the contraction with
 //               the centre's dE/dG on the CUDA cores, and the pair force applied to both atoms in
 //               64-bit fixed point (order-independent sums); k_facc_apply4 adds it to the forces.
@@ -35,7 +36,7 @@
 
 struct NnpTc {
   unsigned long long* d_facc = nullptr;   // network forces and virial [natom][4], fixed point (2^-32)
-  unsigned char* d_fit = nullptr;    // per species: L1 (N128,K256) L2 (128,128) B2 (128,128) B1 (256,128)
+  unsigned char* d_fit = nullptr;    // per species: L1 (N128,K256) and L2 (128,128) images
   size_t fit_stride = 0;
   float* d_emb_small = nullptr;      // per species: W1[32] b1[32] b2[64]
   float* d_fit_small = nullptr;      // per species: c1[128] c2[128] A3[128] c3 (stride 388)
@@ -51,7 +52,7 @@ struct NnpTc {
 namespace {
 
 constexpr int kFitSmallStride = 388;
-constexpr size_t kImgL1 = 128 * 256 * 2, kImgL2 = 128 * 128 * 2, kImgB2 = 128 * 128 * 2, kImgB1 = 256 * 128 * 2;
+constexpr size_t kImgL1 = 128 * 256 * 2, kImgL2 = 128 * 128 * 2;
 
 __device__ __forceinline__ float tanh_fast(float x) {
   float y;
@@ -75,6 +76,11 @@ __device__ __forceinline__ uint32_t mul_bf2(uint32_t a, uint32_t b) {
   uint32_t y;
   asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(y) : "r"(a), "r"(b));
   return y;
+}
+__device__ __forceinline__ uint32_t fma_bf2(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
 }
 
 __device__ __forceinline__ void copy_image(unsigned char* dst, const unsigned char* src, int bytes, int t, int nt) {
@@ -117,7 +123,7 @@ __device__ __forceinline__ void fix_add(unsigned long long* dst, float v) {
 //
 // Per tile t the CTA's 128 threads (row p = thread p) run, in order:
 //   (0) wait for MMA 2 of tile t-1 (its operand buffer and TMEM buffer become free),
-//   (1) warp 0: G of tile t-1 out of TMEM[(t-1) % 2]; all: first layer of tile t+1 into operand
+//   (1) all warps: G of tile t-1 out of TMEM[(t-1) % 2] (16 channels each); first layer of tile t+1 into operand
 //       buffer A[(t+1) % 2], loads of tile t+2 issued,
 //   (2) barrier, after which MMA 1 of tile t is complete,
 //   (3) MMA 1 of tile t+1 into TMEM[(t+1) % 2] (Z = H W2s, K = 64 block-diagonal over the neighbour
@@ -130,7 +136,8 @@ __device__ __forceinline__ void fix_add(unsigned long long* dst, float v) {
 // reads it, and four CTAs per SM overlap each other's waits. The activations are BF16 operands of the next MMA, so their tanh is evaluated on
 // BF16 pairs (one transcendental-unit operation per two values).
 constexpr int kK64 = 64;
-constexpr int kEmbStride4 = 132;   // 16-byte aligned rows of the per-species constants
+constexpr int kEmbStride4 = 148;   // 16-byte aligned rows of the per-species constants: W1[32] b1[32] b2[64], 4 unused, WR[16]
+constexpr int kWrOff = 132;        // WR: w/rc of the first layer as BF16 pairs (the force kernel's r-derivative)
 constexpr int kDescStages = 2;
 constexpr int kSmemDesc2 = 64 * kK64 * 2 + kDescStages * kTile * kK64 * 2 + 8 * kTile * 2 + 2 * kEmbStride4 * 4 + 256 * 4;
 
@@ -242,13 +249,14 @@ __device__ __forceinline__ DescRow desc_first_layer(const DescArgs& d, const Row
   return r;
 }
 
-// Warp 0: G rows (la, s) = lanes 4 la + s of the MMA 2 accumulator at taddr, added to the carried
+// Channels [c0, c0 + 16) of the G rows (la, s) = lanes 4 la + s of this warp's quarter of the MMA 2
+// accumulator (S repeats every 8 rows, so every quarter holds them) at taddr, added to the carried
 // partial of a segment that began in an earlier tile; stored when the atom's last pair was in this
-// tile, else carried.
-__device__ __forceinline__ void desc_readout(const DescArgs& d, uint32_t taddr, const TileSeg& sg, float* sCarry, int lane) {
-  float g[64];
-#pragma unroll
-  for (int c0 = 0; c0 < 64; c0 += 32) tc::tmem_ld16x2(taddr + c0, taddr + c0 + 16, g + c0, g + c0 + 16);
+// tile, else carried. Each of the CTA's four warps takes one 16-channel slice.
+__device__ __forceinline__ void desc_readout(const DescArgs& d, uint32_t taddr, const TileSeg& sg, float* sCarry, int lane,
+                                             int c0) {
+  float g[16];
+  tc::tmem_ld16(taddr, g);
   const int la = lane >> 2, sc = lane & 3;
   const bool mine = lane < 8 && (la == 0 || sg.nb > 0);
   const int atom = sg.a + la;
@@ -256,17 +264,17 @@ __device__ __forceinline__ void desc_readout(const DescArgs& d, uint32_t taddr, 
   const bool done = mine && start + nrow == __ldg(d.n6 + atom);
   if (mine && la == 0 && start > 0) {
 #pragma unroll
-    for (int c = 0; c < 64; ++c) g[c] += sCarry[sc * 64 + c];
+    for (int c = 0; c < 16; ++c) g[c] += sCarry[sc * 64 + c0 + c];
   }
   __syncwarp();
   if (mine) {
     if (done) {   // BF16 (round to nearest), the rounding the fitting kernel's operand takes
-      uint4* dst = reinterpret_cast<uint4*>(d.G2 + (size_t)atom * 128 + sc * 32);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) dst[q] = tc::pack8(g + 8 * q);
+      uint4* dst = reinterpret_cast<uint4*>(d.G2 + (size_t)atom * 128 + sc * 32 + c0 / 2);
+      dst[0] = tc::pack8(g);
+      dst[1] = tc::pack8(g + 8);
     } else {
 #pragma unroll
-      for (int c = 0; c < 64; ++c) sCarry[sc * 64 + c] = g[c];
+      for (int c = 0; c < 16; ++c) sCarry[sc * 64 + c0 + c] = g[c];
     }
   }
   __syncwarp();
@@ -340,8 +348,8 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
       ph_g ^= 1;
       if (!alive) break;
     }
-    // (1) warp 0: G of tile it-1; all: first layer of tile it+1 into A[b1], loads of tile it+2
-    if (havep && w == 0) desc_readout(d, tmem + 64 * b1, segp, sCarry, lane);
+    // (1) all warps: G of tile it-1 (16 channels each), first layer of tile it+1 into A[b1], loads of tile it+2
+    if (havep) desc_readout(d, tmem + 64 * b1 + lane_off + 16 * w, segp, sCarry, lane, 16 * w);
     bool have2 = false;
     seg2 = TileSeg{0, 0, 0, 0};
     if (have1) {
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   // G of the last tile
   if (havep && alive) {
     alive = cta_wait_mma(&bar_g, ph_g, d.ctrl);
-    if (alive && w == 0) desc_readout(d, tmem + 64 * last_buf, segp, sCarry, lane);
+    if (alive) desc_readout(d, tmem + 64 * last_buf + lane_off + 16 * w, segp, sCarry, lane, 16 * w);
   }
   tc::fence_before();
   __syncthreads();
@@ -482,20 +490,26 @@ __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const 
   const float r_rc = 1.f / a.rc, u = r.r * r_rc;
   const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
   const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
+  const uint4* WR = reinterpret_cast<const uint4*>(sE + r.tj * kEmbStride4 + kWrOff);
+  const uint32_t one2 = 0x3F803F80u;   // (1, 1) in BF16
 #pragma unroll
   for (int gg = 0; gg < 2; ++gg) {
     const int g = 2 * half + gg;   // 8-unit chunk
     const float4 w0 = W1[2 * g], w1 = W1[2 * g + 1], b0 = B1[2 * g], b1 = B1[2 * g + 1];
-    const float w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-    const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-    float h[8], v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      h[q] = tanh_fast(fmaf(w[q], u, bb[q]));
-      v[q] = (1.f - h[q] * h[q]) * w[q] * r_rc;
-    }
-    *reinterpret_cast<uint4*>(AH + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = tc::pack8(h);
-    *reinterpret_cast<uint4*>(AV + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = tc::pack8(v);
+    // h on BF16 pairs (it is a BF16 operand), and V = (1 - h^2) w / rc from it on BF16 pairs: one
+    // transcendental-unit operation per two units, the derivative without conversions
+    uint4 h, v;
+    h.x = tanh_bf2(pack_bf2(fmaf(w0.x, u, b0.x), fmaf(w0.y, u, b0.y)));
+    h.y = tanh_bf2(pack_bf2(fmaf(w0.z, u, b0.z), fmaf(w0.w, u, b0.w)));
+    h.z = tanh_bf2(pack_bf2(fmaf(w1.x, u, b1.x), fmaf(w1.y, u, b1.y)));
+    h.w = tanh_bf2(pack_bf2(fmaf(w1.z, u, b1.z), fmaf(w1.w, u, b1.w)));
+    const uint4 wr = WR[g];
+    v.x = mul_bf2(fma_bf2(h.x ^ 0x80008000u, h.x, one2), wr.x);
+    v.y = mul_bf2(fma_bf2(h.y ^ 0x80008000u, h.y, one2), wr.y);
+    v.z = mul_bf2(fma_bf2(h.z ^ 0x80008000u, h.z, one2), wr.z);
+    v.w = mul_bf2(fma_bf2(h.w ^ 0x80008000u, h.w, one2), wr.w);
+    *reinterpret_cast<uint4*>(AH + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = h;
+    *reinterpret_cast<uint4*>(AV + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = v;
     *reinterpret_cast<uint4*>(AH + tc::kmajor_off(p, 32 * (1 - r.tj) + 8 * g, kK64)) = make_uint4(0, 0, 0, 0);
     *reinterpret_cast<uint4*>(AV + tc::kmajor_off(p, 32 * (1 - r.tj) + 8 * g, kK64)) = make_uint4(0, 0, 0, 0);
   }
@@ -540,6 +554,12 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   }
   copy_image(sW, a.wdesc, 64 * kK64 * 2, t, 256);
   for (int k = t; k < 2 * 128; k += 256) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < a.ntype ? a.emb_small[k] : 0.f;
+  for (int k = t; k < 2 * 16; k += 256) {
+    const int sp = k >> 4, q = k & 15;
+    const float r_rc = 1.f / a.rc;
+    const float w0 = sp < a.ntype ? a.emb_small[sp * 128 + 2 * q] : 0.f, w1 = sp < a.ntype ? a.emb_small[sp * 128 + 2 * q + 1] : 0.f;
+    reinterpret_cast<uint32_t*>(sE)[sp * kEmbStride4 + kWrOff + q] = pack_bf2(w0 * r_rc, w1 * r_rc);
+  }
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
@@ -644,16 +664,21 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     sAcc[half * kTile + p] = part;
     fetch_xj(dv, f2, true);
     __syncthreads();
-    // (5) half 0: pair forces to j's owner, per-segment sums for the atoms of the tile
-    if (half == 0) {
+    // (5) both halves form the row's pair force: half 0 applies it to j's owner, half 1 sums it per
+    // atom segment for the atoms of the tile
+    {
       float gx = 0.f, gy = 0.f, gz = 0.f, vr = 0.f;
       if (row0.valid) {
         const float fpair = -(sAcc[p] + sAcc[kTile + p]) / row0.r;
         gx = row0.dx * fpair; gy = row0.dy * fpair; gz = row0.dz * fpair;
         if (EV) vr = fpair * row0.rsq;
-        unsigned long long* fj = a.facc + 4 * (size_t)row0.jo;
-        fix_add(fj, -gx); fix_add(fj + 1, -gy); fix_add(fj + 2, -gz);
       }
+      if (half == 0) {
+        if (row0.valid) {
+          unsigned long long* fj = a.facc + 4 * (size_t)row0.jo;
+          fix_add(fj, -gx); fix_add(fj + 1, -gy); fix_add(fj + 2, -gz);
+        }
+      } else {
       const unsigned in0 = __ballot_sync(0xffffffffu, row0.valid && row0.la == 0);
       const unsigned in1 = __ballot_sync(0xffffffffu, row0.valid && row0.la == 1);
 #pragma unroll
@@ -668,6 +693,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
           fix_add(fi, sx); fix_add(fi + 1, sy2); fix_add(fi + 2, sz);
           if (EV) fix_add(fi + 3, sv);
         }
+      }
       }
     }
     seg0 = seg1; have0 = have1; row0 = row1;
@@ -709,9 +735,10 @@ struct FitTcArgs {
 
 // One MMA chain of the fitting kernel: thread 0 waits for the weight image's bulk copy (wbar,
 // wphase), issues the chain and waits for its completion; false (and NNPE_DEV_TIMEOUT) when either
-// bounded wait gave up.
+// bounded wait gave up. b_mn: the B image is read as an MN-major tile (the transpose of the
+// K-major image of the forward layer: the backward's A^T without a second image).
 __device__ __forceinline__ bool fit_mma(uint32_t tmem, uint32_t aA, int KA, uint32_t aB, int N, uint64_t* bar, uint32_t phase,
-                                        uint64_t* wbar, uint32_t wphase, int t, int* ctrl) {
+                                        uint64_t* wbar, uint32_t wphase, int t, int* ctrl, bool b_mn = false) {
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
@@ -720,8 +747,9 @@ __device__ __forceinline__ bool fit_mma(uint32_t tmem, uint32_t aA, int KA, uint
   if (t == 0) {
     got = tc::mbar_wait(wbar, wphase);
     if (got) {
-      const uint32_t id = tc::idesc_bf16(128, N);
-      for (int kk = 0; kk < KA / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(aA, KA, kk), tc::tile_desc(aB, KA, kk), id, kk > 0);
+      const uint32_t id = tc::idesc_bf16(128, N, b_mn);
+      for (int kk = 0; kk < KA / 16; ++kk)
+        tc::mma_bf16(tmem, tc::tile_desc(aA, KA, kk), b_mn ? tc::tile_desc_mn(aB, N, kk) : tc::tile_desc(aB, KA, kk), id, kk > 0);
       tc::mma_commit(bar);
       got = tc::mbar_wait(bar, phase);
     }
@@ -740,9 +768,10 @@ __device__ __forceinline__ void load_image(unsigned char* dst, const unsigned ch
     tc::bulk_g2s(dst + off, src + off, min(32768u, bytes - off), bar);
 }
 
-// 128 atoms of one species per CTA; the four weight images stream through two shared buffers by
-// bulk copies (one barrier per buffer, two phases each) so that each copy overlaps the MMA chain and
-// epilogue before it. 256 threads: row p = t % 128 (TMEM lane), half h = t / 128 takes half of each
+// 128 atoms of one species per CTA; the two weight images (A1 and A2, K-major) arrive by bulk
+// copies (one barrier each) that overlap the G fetch and the first MMA chain. The backward chains
+// read the same images as MN-major tiles, which are A1^T and A2^T, so no transposed copy is
+// loaded. 256 threads: row p = t % 128 (TMEM lane), half h = t / 128 takes half of each
 // epilogue's columns.
 __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   extern __shared__ __align__(128) unsigned char sm[];
@@ -751,8 +780,8 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   __shared__ float sEn[2][128];             // per-half partial energies
   unsigned char* sAct = sm;                 // 128 x 256 (G), later 128 x 128 (g2)
   unsigned char* sH1 = sm + 128 * 256 * 2;  // 128 x 128 (h1, later g1)
-  unsigned char* sW0 = sH1 + 128 * 128 * 2; // L1, then B2
-  unsigned char* sW1 = sW0 + 128 * 256 * 2; // L2, then B1
+  unsigned char* sW0 = sH1 + 128 * 128 * 2; // L1 image (K-major A1; MN-major it is A1^T for B1)
+  unsigned char* sW1 = sW0 + 128 * 256 * 2; // L2 image (K-major A2; MN-major it is A2^T for B2)
   const int t = threadIdx.x, w = t >> 5, p = t & 127, half = t >> 7;
   const int sp = f.tile_sp[blockIdx.x], row0 = f.tile_row[blockIdx.x];
   const int M = f.soff[sp + 1] - f.soff[sp];
@@ -791,7 +820,6 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   bool ok = true;
   // L1: z1 = G A1 (+c1), h1 = tanh
   ok = fit_mma(tmem, aAct, 256, aW0, 128, &bar, 0, &bar_w[0], 0, t, f.ctrl);
-  if (ok && t == 0) { load_image(sW0, img + kImgL1 + kImgL2, (uint32_t)kImgB2, &bar_w[0]); ++issued0; }   // B2
   if (ok) {
     for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
       float v[16];
@@ -804,10 +832,6 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   }
   // L2: z2 = h1 A2 (+c2), h2 = tanh, E = h2 A3 + c3, g2 = A3 (1-h2^2)
   if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW1, 128, &bar, 1, &bar_w[1], 0, t, f.ctrl);
-  if (ok && t == 0) {   // B1
-    load_image(sW1, img + kImgL1 + kImgL2 + kImgB2, (uint32_t)kImgB1, &bar_w[1]);
-    ++issued1;
-  }
   if (ok) {
     float e = 0.f;
     for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
@@ -825,7 +849,7 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
     sEn[half][p] = e;
   }
   // B2: u = g2 A2^T, g1 = u (1-h1^2)
-  if (ok) ok = fit_mma(tmem, aAct, 128, aW0, 128, &bar, 0, &bar_w[0], 1, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem, aAct, 128, aW1, 128, &bar, 0, &bar_w[1], 0, t, f.ctrl, true);
   if (ok && half == 0 && valid) f.enet[atom] = (double)(sEn[0][p] + sEn[1][p]) + (double)sm_c3[0];
   if (ok) {
     for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
@@ -848,7 +872,7 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
     }
   }
   // B1: dE/dG = g1 A1^T (N = 256)
-  if (ok) ok = fit_mma(tmem, aH1, 128, aW1, 256, &bar, 1, &bar_w[1], 1, t, f.ctrl);
+  if (ok) ok = fit_mma(tmem, aH1, 128, aW0, 256, &bar, 1, &bar_w[0], 0, t, f.ctrl, true);
   if (ok) {
     for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += 16) {
       float v[16];
@@ -924,7 +948,7 @@ int nnp_tc_setup(nnpe_ctx* c) {
       emb_small[s * 128 + 96 + q] = E[eb * s + 64 + 32 * 64 + 32 + q];
     }
   const size_t fb = (size_t)256 * 128 + 128 + 128 * 128 + 128 + 128 + 1;
-  const size_t stride_el = (kImgL1 + kImgL2 + kImgB2 + kImgB1) / 2;
+  const size_t stride_el = (kImgL1 + kImgL2) / 2;
   std::vector<uint16_t> fit(stride_el * T);
   std::vector<float> fit_small((size_t)kFitSmallStride * T, 0.f);
   for (int s = 0; s < T; ++s) {
@@ -933,8 +957,6 @@ int nnp_tc_setup(nnpe_ctx* c) {
     const size_t b = stride_el * s;
     put_image(fit, b, 128, 256, [&](int n, int k) { return A1[k * 128 + n]; });                                  // L1
     put_image(fit, b + kImgL1 / 2, 128, 128, [&](int n, int k) { return A2[k * 128 + n]; });                     // L2
-    put_image(fit, b + (kImgL1 + kImgL2) / 2, 128, 128, [&](int n, int k) { return A2[n * 128 + k]; });          // B2
-    put_image(fit, b + (kImgL1 + kImgL2 + kImgB2) / 2, 256, 128, [&](int n, int k) { return A1[n * 128 + k]; }); // B1
     for (int q = 0; q < 128; ++q) {
       fit_small[kFitSmallStride * s + q] = c1[q];
       fit_small[kFitSmallStride * s + 128 + q] = c2[q];
@@ -960,7 +982,7 @@ int nnp_tc_setup(nnpe_ctx* c) {
   if (int rc = up((void**)&t->d_tile_sp, tsp.data(), tsp.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_tile_row, trow.data(), trow.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_soff, m->soff.data(), m->soff.size() * 4)) return rc;
-  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 2 * 256 * 128 * 2;
+  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + kImgL1 + kImgL2;
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_desc2, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDesc2));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemForce2));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_tc_force2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemForce2));
@@ -973,7 +995,7 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   NnpTc* t = m->tc;
   if (!t) return nnpe_fail(c, NNPE_EARG, "BF16 tensor-core path needs the 1->32->64 / 256->128->128 network");
   const int sms = nnpe_sm_count(c->device);
-  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + 2 * 256 * 128 * 2;
+  const int smem_fit = 128 * 256 * 2 + 128 * 128 * 2 + kImgL1 + kImgL2;
   DescArgs dd;
   dd.pos = c->d_pos; dd.list6 = m->d_list6; dd.n6 = m->d_n6; dd.gowner = c->d_gowner;
   dd.wdesc = t->d_wdesc64; dd.emb_small = t->d_emb_small; dd.G2 = reinterpret_cast<uint32_t*>(m->d_G); dd.ctrl = c->d_ctrl;
