@@ -628,7 +628,9 @@ def main():
             "metric": "replica-steps/s", "value": res["replica_steps_per_s"], "unit": "replica-steps/s", "n_gpus": 1,
             "steps": res["total_steps"], "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded request stream)",
-            "config": {"workload": args.workload, "description": wl["desc"], "serve_scale": args.serve_scale,
+            "config": {"workload": args.workload,
+                       "description": wl["desc"].replace("at 20 req/s", "at %g req/s" % args.serve_rate),
+                       "serve_scale": args.serve_scale,
                        "arrival_rate_per_s": args.serve_rate,
                        "slots": args.serve_slots, "autotune": not args.no_autotune, "timing": "host clock: first arrival to last completion"},
             "latency_s": {"p50": res["p50_s"], "p99": res["p99_s"], "mean": res["mean_s"]},

@@ -44,7 +44,7 @@ static void nfree(T** p) {
 void nnp_free(nnpe_ctx* c) {
   NnpModel* m = c->nnp;
   if (!m) return;
-  nfree(&m->d_embw); nfree(&m->d_fitw); nfree(&m->d_tdesc); nfree(&m->d_tpair); nfree(&m->d_G); nfree(&m->d_dG);
+  nfree(&m->d_embw); nfree(&m->d_fitw); nfree(&m->d_fitg); nfree(&m->d_tdesc); nfree(&m->d_tpair); nfree(&m->d_G); nfree(&m->d_dG);
   nfree(&m->d_enet); nfree(&m->d_list6); nfree(&m->d_n6); nfree(&m->d_sidx); nfree(&m->d_scount);
   nfree(&m->d_H1); nfree(&m->d_G2); nfree(&m->d_G1); nfree(&m->d_soff_dev);
   nnp_tc_free(m);
@@ -115,6 +115,8 @@ static void gen_tables(int npair, float cutoff, int nbin, const float* coef_p_in
 
 static size_t fit_block(int din, int h1, int h2) { return (size_t)din * h1 + h1 + (size_t)h1 * h2 + h2 + h2 + 1; }
 static constexpr int kEmbWarpsHost = 4;
+static constexpr int kDescScratchHost = 32 * 32 + 3 * 32;                     // floats per warp, k_emb_desc_f32
+static constexpr int kForceScratchHost = 16 * (32 + 32 + 33) + 10 * 32;   // floats per warp, k_emb_force_f32
 static int nnp_set_smem_attrs(nnpe_ctx* c, int smem_desc, int smem_force);
 
 int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, int e1, int e2, int h1, int h2,
@@ -152,6 +154,30 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   if ((rc = nalloc(c, &m->d_fitw, fb * c->ntype))) return rc;
   NNPE_CUDA(c, cudaMemcpy(m->d_fitw, fitw, sizeof(float) * fb * c->ntype, cudaMemcpyHostToDevice));
   m->h_fitw.assign(fitw, fitw + fb * c->ntype);
+  {   // aligned copies for the FP32 GEMMs, with the backward's transposed weights
+    const int D = m->din;
+    auto up4 = [](size_t n) { return (n + 3) & ~(size_t)3; };
+    const size_t o2 = up4((size_t)D * h1), o2t = o2 + up4((size_t)h1 * h2), o1t = o2t + up4((size_t)h2 * h1),
+                 oc1 = o1t + up4((size_t)h1 * D), oc2 = oc1 + up4(h1), oa3 = oc2 + up4(h2);
+    m->fitg_block = oa3 + up4(h2);
+    std::vector<float> g(m->fitg_block * c->ntype, 0.f);
+    for (int t = 0; t < c->ntype; ++t) {
+      const float* w = fitw + fb * t;
+      const float *A1 = w, *c1 = A1 + (size_t)D * h1, *A2 = c1 + h1, *c2 = A2 + (size_t)h1 * h2, *A3 = c2 + h2;
+      float* o = g.data() + m->fitg_block * t;
+      std::copy(A1, A1 + (size_t)D * h1, o);
+      std::copy(A2, A2 + (size_t)h1 * h2, o + o2);
+      for (int k = 0; k < h2; ++k)
+        for (int n2 = 0; n2 < h1; ++n2) o[o2t + (size_t)k * h1 + n2] = A2[(size_t)n2 * h2 + k];
+      for (int k = 0; k < h1; ++k)
+        for (int n2 = 0; n2 < D; ++n2) o[o1t + (size_t)k * D + n2] = A1[(size_t)n2 * h1 + k];
+      std::copy(c1, c1 + h1, o + oc1);
+      std::copy(c2, c2 + h2, o + oc2);
+      std::copy(A3, A3 + h2, o + oa3);
+    }
+    if ((rc = nalloc(c, &m->d_fitg, g.size()))) return rc;
+    NNPE_CUDA(c, cudaMemcpy(m->d_fitg, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice));
+  }
   if ((rc = nalloc(c, &m->d_G, (size_t)N * m->din)) || (rc = nalloc(c, &m->d_dG, (size_t)N * m->din)) ||
       (rc = nalloc(c, &m->d_enet, N)) || (rc = nalloc(c, &m->d_list6, (size_t)N * m->cap6)) ||
       (rc = nalloc(c, &m->d_n6, N)) || (rc = nalloc(c, &m->d_sidx, N)) || (rc = nalloc(c, &m->d_scount, NNPE_MAX_TYPES)) ||
@@ -169,9 +195,8 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   NNPE_CUDA(c, cudaMemcpy(m->d_soff_dev, m->soff.data(), sizeof(int) * m->soff.size(), cudaMemcpyHostToDevice));
   if (kind == 1) {
     const size_t eb = (size_t)32 + 32 + 32 * (size_t)e2 + e2;
-    const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * 32 * (e2 + 1) + 32 * kEmbWarpsHost * 32) +
-                                sizeof(int) * kEmbWarpsHost * 32);
-    const int smem_force = (int)(sizeof(float) * (eb * c->ntype + 32 * kEmbWarpsHost * 32));
+    const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * kDescScratchHost));
+    const int smem_force = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * kForceScratchHost));
     if (int r2 = nnp_set_smem_attrs(c, smem_desc, smem_force)) return r2;
   }
   c->graph_valid = false;
@@ -348,204 +373,250 @@ __global__ void __launch_bounds__(128) k_gauss_force(NnpArgs a) {
   }
 }
 
-// First layer h = tanh(W1 u + b1) of the embedding net wt (W1[32] b1[32] W2[32][64] b2[64]) into this
-// thread's shared-memory slots hs[q * h_stride] (the e1 = 32, e2 = 64 network of this path).
-__device__ __forceinline__ void emb_layer1(const float* wt, float u, float* hs, int h_stride) {
-#pragma unroll
-  for (int q = 0; q < 32; ++q) hs[q * h_stride] = tanhf(wt[q] * u + wt[32 + q]);
-}
-// Channels [c0, c0 + 32) of the second layer's pre-activations z = b2 + W2^T h, h from the slots:
-// 32 sums in registers, each W2 row chunk read as 16-byte broadcasts (all lanes read the same row).
-__device__ __forceinline__ void emb_layer2_half(const float* wt, const float* hs, int h_stride, int c0, float* z) {
-  const float4* b2 = reinterpret_cast<const float4*>(wt + 64 + 32 * 64 + c0);
-#pragma unroll
-  for (int c4 = 0; c4 < 8; ++c4) {
-    const float4 b = b2[c4];
-    z[4 * c4] = b.x; z[4 * c4 + 1] = b.y; z[4 * c4 + 2] = b.z; z[4 * c4 + 3] = b.w;
-  }
-#pragma unroll 8
-  for (int q = 0; q < 32; ++q) {
-    const float4* row = reinterpret_cast<const float4*>(wt + 64 + q * 64 + c0);
-    const float hq = hs[q * h_stride];
-#pragma unroll
-    for (int c4 = 0; c4 < 8; ++c4) {
-      const float4 w4 = row[c4];
-      z[4 * c4] += hq * w4.x; z[4 * c4 + 1] += hq * w4.y; z[4 * c4 + 2] += hq * w4.z; z[4 * c4 + 3] += hq * w4.w;
-    }
-  }
-}
-
-// ---- embedding descriptor (FP32): one warp per atom, lanes over pairs; each lane evaluates its
-// pair's e1->e2 embedding with the weights of the neighbour's species from shared memory, then
-// the warp reduces channel sums per special class through shared memory (deterministic order).
+// ---- FP32 embedding network on CUDA cores (the plain form). One warp per atom. Lane l owns output
+// channels 2l and 2l+1, and the warp takes the atom's pairs one neighbour species at a time, so that
+// it holds that species' second-layer weights W2[q][2l], W2[q][2l+1] (64 values) in registers. Per
+// group of up to 32 pairs of the species (ballot-compacted from the list), lane q computes
+// first-layer unit q of every pair into shared memory; then pair by pair every lane reads the pair's
+// 32 first-layer values as 16-byte broadcasts and runs its two channels' sums: one weight register
+// per FMA and no weight traffic, 64 FMAs per lane per pair and layer.
+// The embedding net wt of one species is W1[32] b1[32] W2[32][64] b2[64] (e1 = 32, e2 = 64).
 constexpr int kEmbWarps = 4;
-__global__ void __launch_bounds__(kEmbWarps * 32, 3) k_emb_desc_f32(NnpArgs a) {
-  extern __shared__ float sm[];
-  const int E1 = 32, E2 = a.e2;
-  const size_t eb = (size_t)E1 + E1 + (size_t)E1 * E2 + E2;
-  float* W = sm;                                   // [ntype][eb]
-  float* Y = sm + eb * a.ntype;                    // [warps][32][E2+1]
-  int* S = (int*)(Y + kEmbWarps * 32 * (E2 + 1));  // [warps][32]
-  float* Hs = (float*)(S + kEmbWarps * 32);        // [32][threads]: first-layer values of each thread's pair
-  for (int k = threadIdx.x; k < (int)(eb * a.ntype); k += blockDim.x) W[k] = a.embw[k];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-  const int i = blockIdx.x * kEmbWarps + wi;
-  if (i >= a.N) return;
-  float* Yw = Y + wi * 32 * (E2 + 1);
-  int* Sw = S + wi * 32;
-  const float4 xi = a.pos[i];
-  const uint32_t* row = a.list6 + (size_t)i * a.cap6;
-  const int n = a.n6[i];
-  float acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  const float r_rc = 1.f / a.rc;
-  for (int base = 0; base < n; base += 32) {
-    const int k = base + lane;
-    int s = 0;
-    if (k < n) {
-      const uint32_t ent = row[k];
-      const float4 xj = a.pos[ent & NNPE_J_MASK];
-      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r = sqrtf(dx * dx + dy * dy + dz * dz);
-      const float u = r * r_rc, cf = r - a.rc, cff = a.scale * (1.f - 1.f / (1.f + cf * cf));
-      s = ent >> 30;
-      const float* w = W + eb * ((ent >> 27) & 7);
-      float* hs = Hs + threadIdx.x;
-      emb_layer1(w, u, hs, blockDim.x);
-#pragma unroll
-      for (int c0 = 0; c0 < 64; c0 += 32) {
-        float z[32];
-        emb_layer2_half(w, hs, blockDim.x, c0, z);
-#pragma unroll
-        for (int cc = 0; cc < 32; ++cc) Yw[lane * (E2 + 1) + c0 + cc] = tanhf(z[cc]) * cff;
-      }
-    } else {
-      for (int cc = 0; cc < E2; ++cc) Yw[lane * (E2 + 1) + cc] = 0.f;
-    }
-    Sw[lane] = s;
-    __syncwarp();
-    const int m = min(32, n - base);
-    for (int l = 0; l < m; ++l) {
-      const int sl = Sw[l];
-#pragma unroll
-      for (int h2 = 0; h2 < 2; ++h2) {
-        const int cc = lane + 32 * h2;
-        const float v = cc < E2 ? Yw[l * (E2 + 1) + cc] : 0.f;
-        acc[0][h2] += sl == 0 ? v : 0.f;
-        acc[1][h2] += sl == 1 ? v : 0.f;
-        acc[2][h2] += sl == 2 ? v : 0.f;
-        acc[3][h2] += sl == 3 ? v : 0.f;
-      }
-    }
-    __syncwarp();
-  }
-  float* Gi = a.G + (size_t)i * 4 * E2;
-#pragma unroll
-  for (int s = 0; s < 4; ++s)
-#pragma unroll
-    for (int h2 = 0; h2 < 2; ++h2) {
-      const int cc = lane + 32 * h2;
-      if (cc < E2) Gi[s * E2 + cc] = acc[s][h2];
-    }
+constexpr int kEmbBlock = 32 + 32 + 32 * 64 + 64;
+
+// tanh(x) = 1 - 2 / (exp(2x) + 1), with the exponential as 2^(2 x log2 e) on the hardware base-2
+// unit and the quotient on the hardware reciprocal: absolute error a few 1e-7, saturating exactly
+// (the exponential overflows to +inf -> 1, underflows to 0 -> -1).
+__device__ __forceinline__ float tanh_fast(float x) {
+  float e, r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(x * 2.8853900817779268f));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e + 1.f));
+  return fmaf(-2.f, r, 1.f);
 }
 
-// ---- embedding force (FP32): recompute the pair's embedding, back-propagate
-// a_c = scale*(dE/dG_i + dE/dG_j)[s*e2+c] through it to dE/dr, fpair = -dE/dr / r.
-// d/dr of sum_c scale * (ga + gb)[c] * y_c(r) * cff(r) for the embedding net wt (W1 b1 W2 b2).
-// Register-blocked: the 64 second-layer values of a pair live in registers and every W2 row is read
-// as 16-byte broadcasts (all lanes of a warp read the same row), four FMAs per shared-memory load.
-// hs: this thread's slots for the 32 first-layer values in shared memory (stride h_stride), kept
-// there across the backward so that the 64 channel values and the row sums fit in registers.
-__device__ __forceinline__ float emb_dedr(const float* wt, int E2, float u, float r_rc, float cff, float dcff,
-                                          float scale, const float* ga, const float* gb, float* hs, int h_stride) {
-  emb_layer1(wt, u, hs, h_stride);
-  float t[32];
-#pragma unroll
-  for (int q = 0; q < 32; ++q) t[q] = 0.f;
-  float dEdr = 0.f;
-#pragma unroll
-  for (int c0 = 0; c0 < 64; c0 += 32) {   // 32 channels at a time: their z, then their share of t
-    float g[32];
-    emb_layer2_half(wt, hs, h_stride, c0, g);
-#pragma unroll
-    for (int cc = 0; cc < 32; cc += 4) {
-      float4 a4 = *reinterpret_cast<const float4*>(ga + c0 + cc);
-      if (gb) {
-        const float4 b4 = *reinterpret_cast<const float4*>(gb + c0 + cc);
-        a4.x += b4.x; a4.y += b4.y; a4.z += b4.z; a4.w += b4.w;
-      }
-      const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float y = tanhf(g[cc + e]);
-        const float ac = scale * av[e];
-        dEdr += ac * y * dcff;
-        g[cc + e] = ac * cff * (1.f - y * y);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 32; ++q) {
-      const float4* row = reinterpret_cast<const float4*>(wt + 64 + q * 64 + c0);
-      float t0 = 0.f, t1 = 0.f;
-#pragma unroll
-      for (int c4 = 0; c4 < 8; c4 += 2) {
-        const float4 w4 = row[c4], w5 = row[c4 + 1];
-        t0 += g[4 * c4] * w4.x + g[4 * c4 + 1] * w4.y + g[4 * c4 + 2] * w4.z + g[4 * c4 + 3] * w4.w;
-        t1 += g[4 * c4 + 4] * w5.x + g[4 * c4 + 5] * w5.y + g[4 * c4 + 6] * w5.z + g[4 * c4 + 7] * w5.w;
-      }
-      t[q] += t0 + t1;
-    }
-  }
+// One species' embedding weights as lane l holds them.
+struct EmbLane {
+  float wa[32], wb[32];   // W2[q][2l], W2[q][2l + 1]
+  float w1, b1, w1r;      // first-layer unit q = l: W1[l], b1[l], W1[l] / rc
+  float b2a, b2b;         // b2[2l], b2[2l + 1]
+};
+__device__ __forceinline__ void emb_lane_load(const float* wt, int lane, float r_rc, EmbLane& L) {
+  L.w1 = wt[lane];
+  L.b1 = wt[32 + lane];
+  L.w1r = L.w1 * r_rc;
 #pragma unroll
   for (int q = 0; q < 32; ++q) {
-    const float hq = hs[q * h_stride];
-    dEdr += t[q] * (1.f - hq * hq) * wt[q] * r_rc;
+    const float2 w = *reinterpret_cast<const float2*>(wt + 64 + q * 64 + 2 * lane);
+    L.wa[q] = w.x;
+    L.wb[q] = w.y;
   }
-  return dEdr;
+  const float2 b = *reinterpret_cast<const float2*>(wt + 64 + 32 * 64 + 2 * lane);
+  L.b2a = b.x;
+  L.b2b = b.y;
 }
 
-template <bool EV>
-__global__ void __launch_bounds__(kEmbWarps * 32, 3) k_emb_force_f32(NnpArgs a) {
-  extern __shared__ float sm[];
-  const int E1 = 32, E2 = a.e2;
-  const size_t eb = (size_t)E1 + E1 + (size_t)E1 * E2 + E2;
-  float* W = sm;
-  float* Hs = sm + eb * a.ntype;   // [32][threads]: first-layer values of each thread's pair
-  for (int k = threadIdx.x; k < (int)(eb * a.ntype); k += blockDim.x) W[k] = a.embw[k];
+// za += sum_q W2[q][2l] h_q, zb += sum_q W2[q][2l + 1] h_q over one pair's row h (32 first-layer
+// values, 16-byte aligned in shared memory, read as broadcasts), q in order.
+__device__ __forceinline__ void emb_row(const EmbLane& L, const float* h, float& za, float& zb) {
+  const float4* h4 = reinterpret_cast<const float4*>(h);
+#pragma unroll
+  for (int q4 = 0; q4 < 8; ++q4) {
+    const float4 v = h4[q4];
+    za = fmaf(L.wa[4 * q4], v.x, za); zb = fmaf(L.wb[4 * q4], v.x, zb);
+    za = fmaf(L.wa[4 * q4 + 1], v.y, za); zb = fmaf(L.wb[4 * q4 + 1], v.y, zb);
+    za = fmaf(L.wa[4 * q4 + 2], v.z, za); zb = fmaf(L.wb[4 * q4 + 2], v.z, zb);
+    za = fmaf(L.wa[4 * q4 + 3], v.w, za); zb = fmaf(L.wb[4 * q4 + 3], v.w, zb);
+  }
+}
+
+// acc[s] += (ya, yb) for a warp-uniform special class s.
+__device__ __forceinline__ void add_class(float (&acc)[4][2], int s, float ya, float yb) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (s == c) { acc[c][0] += ya; acc[c][1] += yb; }
+}
+
+// ---- embedding descriptor (FP32): G_i[s][c] = sum over the pairs of class s of scale cff(r) y_c(r),
+// y = tanh(b2 + W2^T tanh(W1 u + b1)) of the neighbour's species, u = r / rc. Sums per lane in a fixed
+// order (species by species, list order within), so deterministic.
+// Shared memory per warp (kDescScratch floats): first-layer rows [32][32], then per pair u, scale cff, s.
+constexpr int kDescScratch = 32 * 32 + 3 * 32;
+__global__ void __launch_bounds__(kEmbWarps * 32, 4) k_emb_desc_f32(NnpArgs a) {
+  extern __shared__ __align__(16) float sm[];
+  float* W = sm;   // [ntype][kEmbBlock]
+  for (int k = threadIdx.x; k < kEmbBlock * a.ntype; k += blockDim.x) W[k] = a.embw[k];
   __syncthreads();
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   const int i = blockIdx.x * kEmbWarps + wi;
   if (i >= a.N) return;
+  float* hb = sm + kEmbBlock * a.ntype + wi * kDescScratch;
+  float* su = hb + 32 * 32;
+  float* scs = su + 32;
+  int* ss = reinterpret_cast<int*>(scs + 32);
   const float4 xi = a.pos[i];
   const uint32_t* row = a.list6 + (size_t)i * a.cap6;
   const int n = a.n6[i];
-  const float* dGi = a.dG + (size_t)i * 4 * E2;
+  const float r_rc = 1.f / a.rc;
+  float acc[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+  for (int t = 0; t < a.ntype; ++t) {
+    EmbLane L;
+    bool loaded = false;
+    for (int base = 0; base < n; base += 32) {
+      const int k = base + lane;
+      const uint32_t ent = k < n ? row[k] : 0u;
+      const bool sel = k < n && (int)((ent >> 27) & 7) == t;
+      const unsigned mask = __ballot_sync(0xffffffffu, sel);
+      if (!mask) continue;   // warp-uniform
+      if (!loaded) { emb_lane_load(W + kEmbBlock * t, lane, r_rc, L); loaded = true; }
+      const int m = __popc(mask);
+      if (sel) {
+        const int rk = __popc(mask & ((1u << lane) - 1u));
+        const float4 xj = a.pos[ent & NNPE_J_MASK];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        const float cf = r - a.rc;
+        su[rk] = r * r_rc;
+        scs[rk] = a.scale * (1.f - 1.f / (1.f + cf * cf));
+        ss[rk] = (int)(ent >> 30);
+      }
+      __syncwarp();
+      for (int p = 0; p < m; ++p) hb[p * 32 + lane] = tanh_fast(fmaf(L.w1, su[p], L.b1));
+      __syncwarp();
+      for (int p = 0; p < m; p += 2) {   // two pairs at a time (four independent sums); a lone last pair is doubled
+        const int p1 = min(p + 1, m - 1);
+        float z0 = L.b2a, z1 = L.b2b, z2 = L.b2a, z3 = L.b2b;
+        emb_row(L, hb + p * 32, z0, z1);
+        emb_row(L, hb + p1 * 32, z2, z3);
+        const float c0 = scs[p];
+        add_class(acc, ss[p], tanh_fast(z0) * c0, tanh_fast(z1) * c0);
+        if (p + 1 < m) {
+          const float c1 = scs[p1];
+          add_class(acc, ss[p1], tanh_fast(z2) * c1, tanh_fast(z3) * c1);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  float* Gi = a.G + (size_t)i * 256;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) *reinterpret_cast<float2*>(Gi + s * 64 + 2 * lane) = make_float2(acc[s][0], acc[s][1]);
+}
+
+// ---- embedding force (FP32): per pair (i, j) of i's full list, fpair = -dE/dr / r from the pair's
+// two descriptor terms, applied to i only (a warp-level gather, no atomics):
+//   the term in G_i, through the net of j's species with dE/dG_i, and
+//   the term in G_j, through the net of i's species with dE/dG_j,
+// dE/dr = scale sum_c D_c [dcff y_c + cff (1 - y_c^2) k_c], k_c = sum_q W2[q][c] (1 - h_q^2) W1[q] / rc.
+// Pass t = species of i evaluates that net once per pair with D = dE/dG_j (+ dE/dG_i when j has the
+// same species); a pass t != species of i evaluates it on the pairs whose j is of species t with
+// D = dE/dG_i. Each lane leaves its two channels' share of dE/dr in shared memory; the lane that
+// owns the pair adds the 32 shares in a fixed order.
+// Shared memory per warp (kForceScratch floats): h rows [16][32], dh/dr rows [16][32], shares
+// [16][33] of a group of up to 16 pairs, then per pair of the 32-entry chunk u, scale cff, scale dcff,
+// dx, dy, dz, rsq, r, dE/dG_j row offset, flags.
+constexpr int kForceGroup = 16;
+constexpr int kForceScratch = kForceGroup * (32 + 32 + 33) + 10 * 32;
+template <bool EV>
+__global__ void __launch_bounds__(kEmbWarps * 32, 4) k_emb_force_f32(NnpArgs a) {
+  extern __shared__ __align__(16) float sm[];
+  float* W = sm;
+  for (int k = threadIdx.x; k < kEmbBlock * a.ntype; k += blockDim.x) W[k] = a.embw[k];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int i = blockIdx.x * kEmbWarps + wi;
+  if (i >= a.N) return;
+  float* hb = sm + kEmbBlock * a.ntype + wi * kForceScratch;
+  float* gb = hb + kForceGroup * 32;
+  float* vb = gb + kForceGroup * 32;
+  float* su = vb + kForceGroup * 33;
+  float* scf = su + 32;
+  float* sdcf = scf + 32;
+  float* sdx = sdcf + 32;
+  float* sdy = sdx + 32;
+  float* sdz = sdy + 32;
+  float* srsq = sdz + 32;
+  float* sr = srsq + 32;
+  int* sjo = reinterpret_cast<int*>(sr + 32);
+  int* sfl = sjo + 32;
+  const float4 xi = a.pos[i];
+  const uint32_t* row = a.list6 + (size_t)i * a.cap6;
+  const int n = a.n6[i];
   const int ti = a.info[i].y & 0xFF;
   const float r_rc = 1.f / a.rc;
-  float fx = 0, fy = 0, fz = 0;
-  double w = 0;
-  for (int k = lane; k < n; k += 32) {
-    const uint32_t ent = row[k];
-    const int j = ent & NNPE_J_MASK;
-    const float4 xj = a.pos[j];
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float rsq = dx * dx + dy * dy + dz * dz;
-    const float r = sqrtf(rsq);
-    const float u = r * r_rc, cf = r - a.rc, den = 1.f + cf * cf;
-    const float cff = 1.f - 1.f / den, dcff = 2.f * cf / (den * den);
-    const int s = ent >> 30, tj = (ent >> 27) & 7;
-    const float* dGj = a.dG + (size_t)owner_of(j, a.N, a.gowner) * 4 * E2 + s * E2;
-    const float* dGis = dGi + s * E2;
-    // the pair sits in G_i through the net of t_j and in G_j through the net of t_i (one net
-    // evaluation with the two dE/dG rows added when the species agree)
-    float dEdr = 0.f;
-    const int ndir = tj == ti ? 1 : 2;
-    for (int dir = 0; dir < ndir; ++dir)
-      dEdr += emb_dedr(W + eb * (dir ? ti : tj), E2, u, r_rc, cff, dcff, a.scale, dir ? dGj : dGis,
-                       ndir == 1 ? dGj : nullptr, Hs + threadIdx.x, blockDim.x);
-    const float fpair = -dEdr / r;
-    fx += dx * fpair; fy += dy * fpair; fz += dz * fpair;
-    if (EV) w += 0.5 * (double)(fpair * rsq);
+  const float2* dGi = reinterpret_cast<const float2*>(a.dG + (size_t)i * 256) + lane;   // this lane's channels
+  const float2 Di0 = dGi[0], Di1 = dGi[32], Di2 = dGi[64], Di3 = dGi[96];
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  double w = 0.0;
+  for (int t = 0; t < a.ntype; ++t) {
+    const bool own = t == ti;
+    EmbLane L;
+    bool loaded = false;
+    for (int base = 0; base < n; base += 32) {
+      const int k = base + lane;
+      const uint32_t ent = k < n ? row[k] : 0u;
+      const int tj = (int)((ent >> 27) & 7);
+      const bool sel = k < n && (own || tj == t);
+      const unsigned mask = __ballot_sync(0xffffffffu, sel);
+      if (!mask) continue;   // warp-uniform
+      if (!loaded) { emb_lane_load(W + kEmbBlock * t, lane, r_rc, L); loaded = true; }
+      const int m = __popc(mask);
+      if (sel) {
+        const int rk = __popc(mask & ((1u << lane) - 1u));
+        const int j = ent & NNPE_J_MASK;
+        const float4 xj = a.pos[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float rsq = dx * dx + dy * dy + dz * dz;
+        const float r = sqrtf(rsq);
+        const float cf = r - a.rc, den = 1.f + cf * cf;
+        const int s = (int)(ent >> 30);
+        su[rk] = r * r_rc;
+        scf[rk] = a.scale * (1.f - 1.f / den);
+        sdcf[rk] = a.scale * (2.f * cf / (den * den));
+        sdx[rk] = dx; sdy[rk] = dy; sdz[rk] = dz; srsq[rk] = rsq; sr[rk] = r;
+        sjo[rk] = own ? owner_of(j, a.N, a.gowner) * 256 + s * 64 : 0;
+        sfl[rk] = s | ((own && tj == ti) ? 4 : 0) | (own ? 8 : 0);
+      }
+      __syncwarp();
+      for (int g0 = 0; g0 < m; g0 += kForceGroup) {   // groups of up to 16 of the chunk's pairs
+        const int mg = min(kForceGroup, m - g0);
+        for (int p = 0; p < mg; ++p) {
+          const float h = tanh_fast(fmaf(L.w1, su[g0 + p], L.b1));
+          hb[p * 32 + lane] = h;
+          gb[p * 32 + lane] = (1.f - h * h) * L.w1r;
+        }
+        __syncwarp();
+        for (int p = 0; p < mg; ++p) {
+          const int fl = sfl[g0 + p];
+          float2 D = make_float2(0.f, 0.f);
+          if (fl & 8) D = *reinterpret_cast<const float2*>(a.dG + sjo[g0 + p] + 2 * lane);
+          if (!(fl & 8) || (fl & 4)) {
+            const int sc = fl & 3;
+            const float2 d = sc == 0 ? Di0 : sc == 1 ? Di1 : sc == 2 ? Di2 : Di3;
+            D.x += d.x;
+            D.y += d.y;
+          }
+          float z0 = L.b2a, z1 = L.b2b, k0 = 0.f, k1 = 0.f;
+          emb_row(L, hb + p * 32, z0, z1);
+          emb_row(L, gb + p * 32, k0, k1);
+          const float y0 = tanh_fast(z0), y1 = tanh_fast(z1);
+          const float c = scf[g0 + p], dc = sdcf[g0 + p];
+          vb[p * 33 + lane] = D.x * fmaf(c * (1.f - y0 * y0), k0, dc * y0) + D.y * fmaf(c * (1.f - y1 * y1), k1, dc * y1);
+        }
+        __syncwarp();
+        if (lane < mg) {
+          const int q = g0 + lane;
+          float T = 0.f;
+#pragma unroll 8
+          for (int l = 0; l < 32; ++l) T += vb[lane * 33 + l];
+          const float fpair = -T / sr[q];
+          fx += sdx[q] * fpair;
+          fy += sdy[q] * fpair;
+          fz += sdz[q] * fpair;
+          if (EV) w += 0.5 * (double)(fpair * srsq[q]);
+        }
+        __syncwarp();
+      }
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     fx += __shfl_xor_sync(0xffffffffu, fx, o);
@@ -652,10 +723,115 @@ __global__ void __launch_bounds__(256) k_fit_gemm(FitArgs f) {
   }
 }
 
+// The same four GEMMs with a 64-row x 128-column block tile for K and N multiples of 4 (B row-major
+// [K][N]; the backward's transposed weights are kept as their own row-major copies). 256 threads,
+// each 8 rows x 4 columns; the A tile stays row-major in shared memory and every thread reads 4 k of
+// one row as a 16-byte broadcast (its warp shares its rows), the B tile 4 columns as one 16-byte
+// load: 12 shared-memory loads per 128 FMAs. The next K chunk is loaded into registers while the
+// current one is multiplied.
+constexpr int kFgRows = 64, kFgK = 32, kFgAStride = kFgK + 4, kFgBStride = 128 + 4;
+template <int EPI>
+__global__ void __launch_bounds__(256, 2) k_fit_gemm64(FitArgs f) {
+  __shared__ __align__(16) float As[kFgRows * kFgAStride];
+  __shared__ __align__(16) float Bs[kFgK * kFgBStride];
+  const int t = threadIdx.x, tr = t >> 5, tc = t & 31;   // rows 8 tr .. 8 tr + 7, columns 4 tc .. 4 tc + 3
+  const int row0 = blockIdx.x * kFgRows, col0 = blockIdx.y * 128;
+  // loaders: A as 2 float4 per thread (row e / 8, k quad e % 8), B as 4 float4 (k e / 32, column quad e % 32)
+  int asrc[2];
+  bool aval[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int gr = row0 + (t >> 3) + 32 * u;
+    aval[u] = gr < f.M;
+    asrc[u] = aval[u] ? (f.gatherA ? f.idx[gr] : gr) : 0;
+  }
+  const int akq = (t & 7) * 4, bn = (t & 31) * 4;
+  const bool bval = col0 + bn < f.N;
+  float4 ra[2], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      ra[u] = (aval[u] && k0 + akq < f.K) ? *reinterpret_cast<const float4*>(f.A + (size_t)asrc[u] * f.K + k0 + akq)
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = (t >> 5) + 8 * u;
+      rb[u] = (bval && k0 + k < f.K) ? *reinterpret_cast<const float4*>(f.B + (size_t)(k0 + k) * f.N + col0 + bn)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  load(0);
+  for (int k0 = 0; k0 < f.K; k0 += kFgK) {
+#pragma unroll
+    for (int u = 0; u < 2; ++u) *reinterpret_cast<float4*>(As + ((t >> 3) + 32 * u) * kFgAStride + akq) = ra[u];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) *reinterpret_cast<float4*>(Bs + ((t >> 5) + 8 * u) * kFgBStride + bn) = rb[u];
+    __syncthreads();
+    if (k0 + kFgK < f.K) load(k0 + kFgK);
+    const int kn = min(kFgK, f.K - k0);
+    for (int k = 0; k < kn; k += 4) {
+      float4 a4[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a4[i] = *reinterpret_cast<const float4*>(As + (tr * 8 + i) * kFgAStride + k);
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const float4 b = *reinterpret_cast<const float4*>(Bs + (k + kk) * kFgBStride + tc * 4);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float av = kk == 0 ? a4[i].x : kk == 1 ? a4[i].y : kk == 2 ? a4[i].z : a4[i].w;
+          acc[i][0] = fmaf(av, b.x, acc[i][0]);
+          acc[i][1] = fmaf(av, b.y, acc[i][1]);
+          acc[i][2] = fmaf(av, b.z, acc[i][2]);
+          acc[i][3] = fmaf(av, b.w, acc[i][3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int gc = col0 + tc * 4;
+  const bool cval = gc < f.N;
+  float4 bias = make_float4(0.f, 0.f, 0.f, 0.f), a3 = bias;
+  if (cval && (EPI == EPI_L1 || EPI == EPI_L2)) bias = *reinterpret_cast<const float4*>(f.bias + gc);
+  if (cval && EPI == EPI_L2) a3 = *reinterpret_cast<const float4*>(f.a3 + gc);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gr = row0 + tr * 8 + i;
+    float v[4] = {acc[i][0], acc[i][1], acc[i][2], acc[i][3]};
+    float epart = 0.f;
+    if (gr < f.M && cval) {
+      if (EPI == EPI_L1) {
+        v[0] = tanhf(v[0] + bias.x); v[1] = tanhf(v[1] + bias.y); v[2] = tanhf(v[2] + bias.z); v[3] = tanhf(v[3] + bias.w);
+        *reinterpret_cast<float4*>(f.C + (size_t)gr * f.N + gc) = make_float4(v[0], v[1], v[2], v[3]);
+      } else if (EPI == EPI_L2) {
+        const float h0 = tanhf(v[0] + bias.x), h1 = tanhf(v[1] + bias.y), h2 = tanhf(v[2] + bias.z), h3 = tanhf(v[3] + bias.w);
+        epart = h0 * a3.x + h1 * a3.y + h2 * a3.z + h3 * a3.w;
+        *reinterpret_cast<float4*>(f.C + (size_t)gr * f.N + gc) =
+            make_float4(a3.x * (1.f - h0 * h0), a3.y * (1.f - h1 * h1), a3.z * (1.f - h2 * h2), a3.w * (1.f - h3 * h3));
+      } else if (EPI == EPI_B2) {
+        const float4 h = *reinterpret_cast<const float4*>(f.aux + (size_t)gr * f.N + gc);
+        *reinterpret_cast<float4*>(f.C + (size_t)gr * f.N + gc) =
+            make_float4(v[0] * (1.f - h.x * h.x), v[1] * (1.f - h.y * h.y), v[2] * (1.f - h.z * h.z), v[3] * (1.f - h.w * h.w));
+      } else {
+        *reinterpret_cast<float4*>(f.C + (size_t)f.idx[gr] * f.N + gc) = make_float4(v[0], v[1], v[2], v[3]);
+      }
+    }
+    if (EPI == EPI_L2) {   // the warp holds row gr's 128 columns: energy in a fixed shuffle order
+      for (int o = 16; o > 0; o >>= 1) epart += __shfl_xor_sync(0xffffffffu, epart, o);
+      if (tc == 0 && gr < f.M) f.enet[f.idx[gr]] = (double)epart + (double)f.c3[0];
+    }
+  }
+}
+
 }  // namespace
 
 static int nnp_set_smem_attrs(nnpe_ctx* c, int smem_desc, int smem_force) {
-  static_assert(kEmbWarps == kEmbWarpsHost, "warp count");
+  static_assert(kEmbWarps == kEmbWarpsHost && kDescScratch == kDescScratchHost && kForceScratch == kForceScratchHost,
+                "shared-memory layout of the FP32 embedding kernels");
   NNPE_CUDA(c, cudaFuncSetAttribute(k_emb_desc_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_desc));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_emb_force_f32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_emb_force_f32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_force));
@@ -677,6 +853,8 @@ static NnpArgs make_args(nnpe_ctx* c) {
 static int fit_f32_enqueue(nnpe_ctx* c) {
   NnpModel* m = c->nnp;
   const size_t fb = fit_block(m->din, m->h1, m->h2);
+  const bool wide = m->din % 4 == 0 && m->h1 % 4 == 0 && m->h2 % 4 == 0 && m->h2 <= 128;
+  auto up4 = [](size_t n) { return (n + 3) & ~(size_t)3; };
   for (int t = 0; t < c->ntype; ++t) {
     const int M = m->soff[t + 1] - m->soff[t];
     if (!M) continue;
@@ -688,13 +866,28 @@ static int fit_f32_enqueue(nnpe_ctx* c) {
     float* G2 = m->d_G2 + (size_t)m->soff[t] * m->h2;
     float* G1 = m->d_G1 + (size_t)m->soff[t] * m->h1;
     FitArgs f{};
-    f.idx = idx; f.M = M;
+    f.idx = idx; f.M = M; f.c3 = c3; f.enet = m->d_enet;
+    if (wide) {
+      const float* g = m->d_fitg + m->fitg_block * t;
+      const size_t o2 = up4((size_t)m->din * m->h1), o2t = o2 + up4((size_t)m->h1 * m->h2),
+                   o1t = o2t + up4((size_t)m->h2 * m->h1), oc1 = o1t + up4((size_t)m->h1 * m->din),
+                   oc2 = oc1 + up4(m->h1), oa3 = oc2 + up4(m->h2);
+      const int gm = nblocks(M, kFgRows);
+      f.A = m->d_G; f.K = m->din; f.B = g; f.N = m->h1; f.bias = g + oc1; f.C = H1; f.gatherA = true;
+      k_fit_gemm64<EPI_L1><<<dim3(gm, nblocks(m->h1, 128)), 256, 0, c->stream>>>(f);
+      f.A = H1; f.K = m->h1; f.B = g + o2; f.N = m->h2; f.bias = g + oc2; f.C = G2; f.gatherA = false; f.a3 = g + oa3;
+      k_fit_gemm64<EPI_L2><<<dim3(gm, 1), 256, 0, c->stream>>>(f);
+      f.A = G2; f.K = m->h2; f.B = g + o2t; f.N = m->h1; f.aux = H1; f.C = G1;
+      k_fit_gemm64<EPI_B2><<<dim3(gm, nblocks(m->h1, 128)), 256, 0, c->stream>>>(f);
+      f.A = G1; f.K = m->h1; f.B = g + o1t; f.N = m->din; f.C = m->d_dG;
+      k_fit_gemm64<EPI_B1><<<dim3(gm, nblocks(m->din, 128)), 256, 0, c->stream>>>(f);
+      continue;
+    }
     dim3 g1(nblocks(M, 32), nblocks(m->h1, 128));
     f.A = m->d_G; f.K = m->din; f.B = A1; f.N = m->h1; f.bias = c1; f.C = H1; f.gatherA = true; f.transB = false;
     k_fit_gemm<EPI_L1><<<g1, 256, 0, c->stream>>>(f);
     dim3 g2(nblocks(M, 32), nblocks(m->h2, 128));
-    f.A = H1; f.K = m->h1; f.B = A2; f.N = m->h2; f.bias = c2; f.C = G2; f.gatherA = false; f.a3 = A3; f.c3 = c3;
-    f.enet = m->d_enet;
+    f.A = H1; f.K = m->h1; f.B = A2; f.N = m->h2; f.bias = c2; f.C = G2; f.gatherA = false; f.a3 = A3;
     k_fit_gemm<EPI_L2><<<g2, 256, 0, c->stream>>>(f);
     dim3 g3(nblocks(M, 32), nblocks(m->h1, 128));
     f.A = G2; f.K = m->h2; f.B = A2; f.N = m->h1; f.transB = true; f.aux = H1; f.C = G1;
@@ -731,9 +924,7 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   if (m->kind == 0) {
     k_gauss_desc<<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
   } else {
-    const size_t eb = (size_t)32 + 32 + 32 * (size_t)m->e2 + m->e2;
-    const size_t smem = sizeof(float) * (eb * c->ntype + kEmbWarps * 32 * (m->e2 + 1) + 32 * kEmbWarps * 32) +
-                        sizeof(int) * kEmbWarps * 32;
+    const size_t smem = sizeof(float) * ((size_t)kEmbBlock * c->ntype + kEmbWarps * kDescScratch);
     k_emb_desc_f32<<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
   }
   if (int rc = fit_f32_enqueue(c)) return rc;
@@ -741,8 +932,7 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
     if (ev) k_gauss_force<true><<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
     else k_gauss_force<false><<<nblocks((long)N * 32, 128), 128, 0, st>>>(a);
   } else {
-    const size_t eb = (size_t)32 + 32 + 32 * (size_t)m->e2 + m->e2;
-    const size_t smem = sizeof(float) * (eb * c->ntype + 32 * kEmbWarps * 32);
+    const size_t smem = sizeof(float) * ((size_t)kEmbBlock * c->ntype + kEmbWarps * kForceScratch);
     if (ev) k_emb_force_f32<true><<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
     else k_emb_force_f32<false><<<nblocks(N, kEmbWarps), kEmbWarps * 32, smem, st>>>(a);
   }

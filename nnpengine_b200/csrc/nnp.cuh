@@ -16,6 +16,8 @@ struct NnpModel {
   bool enabled = true;
   float* d_embw = nullptr;   // per species: W1[e1] b1[e1] W2[e1][e2] b2[e2]
   float* d_fitw = nullptr;   // per species: A1[din][h1] c1 A2[h1][h2] c2 A3[h2] c3
+  float* d_fitg = nullptr;   // per species, 16-byte aligned parts: A1 A2 A2^T A1^T c1 c2 A3 (FP32 GEMMs)
+  size_t fitg_block = 0;     // floats per species in d_fitg
   float2* d_tdesc = nullptr; // gauss: (desc, f_desc) [npair][80][nbin+1]
   float2* d_tpair = nullptr; // gauss: (U, F/r) [npair][4][nbin+1]
   float *d_G = nullptr, *d_dG = nullptr;   // [N][din] sorted order
