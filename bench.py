@@ -772,22 +772,21 @@ def main():
     if not args.no_e2e:
         import ctypes as C
         n3 = s.natom * 3
-        x_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
         f_host = torch.empty(n3, dtype=torch.float32, pin_memory=True)
         x0, v0 = x_e2e0, v_e2e0
         erg = C.c_double(0)
         e2e_steps = max(10, args.steps // 4)
-        xs = [(x0 + np.float32(k * 0.5) * v0).ravel() for k in range(e2e_steps + 3)]
+        # each step's positions in their own pinned host buffer, as a host run loop holds its state
+        xs = [torch.from_numpy((x0 + np.float32(k * 0.5) * v0).ravel().astype(np.float32)).pin_memory()
+              for k in range(e2e_steps + 3)]
         for k in range(3):
-            x_host.numpy()[:] = xs[k]
-            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), None, None))
+            e._ok(e.lib.nnpe_force_step(e.h, xs[k].data_ptr(), f_host.data_ptr(), None, None))
         torch.cuda.synchronize()
         nb_e2e0 = e.list_info()["nbuild"]
         h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         h0.record(stream)
         for k in range(e2e_steps):   # forces every step; the energy only on log steps, as run.cpp:309-342
-            x_host.numpy()[:] = xs[3 + k]
-            e._ok(e.lib.nnpe_force_step(e.h, x_host.data_ptr(), f_host.data_ptr(), None, None))
+            e._ok(e.lib.nnpe_force_step(e.h, xs[3 + k].data_ptr(), f_host.data_ptr(), None, None))
         h1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(h0.elapsed_time(h1), dist) / e2e_steps
