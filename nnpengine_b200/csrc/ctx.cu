@@ -91,7 +91,10 @@ int nnpe_create(int device, nnpe_ctx** out) {
 static void free_graphs(nnpe_ctx* c) {
   for (auto& g : c->graph_exec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& g : c->fs_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   c->graph_valid = false;
+  c->fs_valid = false;
 }
 
 static void free_state(nnpe_ctx* c) {
@@ -442,6 +445,7 @@ int nnpe_pair_set_table(nnpe_ctx* c, int nbin, const float* force, const float* 
   NNPE_CUDA(c, cudaMemcpy(c->d_table, t.data(), sizeof(float2) * t.size(), cudaMemcpyHostToDevice));
   c->nbin = nbin;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
@@ -458,6 +462,7 @@ int nnpe_pair_exact(nnpe_ctx* c, int on) {
   if (!c) return NNPE_EARG;
   c->exact_forces = on != 0;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
@@ -465,6 +470,7 @@ int nnpe_pair_enable(nnpe_ctx* c, int on) {
   if (!c) return NNPE_EARG;
   c->pair_on = on != 0;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
@@ -548,6 +554,7 @@ int nnpe_bonded_set(nnpe_ctx* c, int nbond, const int* bonds, int nbtyp, const f
   TRY(up(&c->d_dcoef, dcoef, dcoef ? ndtyp : 0));
   c->nbtyp = nbtyp; c->natyp = natyp; c->ndtyp = ndtyp;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
@@ -571,6 +578,7 @@ int nnpe_verlet_setup(nnpe_ctx* c, double dt, int fp64_state) {
   c->dt = dt;
   c->fp64_state = fp64_state != 0;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
@@ -579,6 +587,7 @@ int nnpe_thermostat(nnpe_ctx* c, int kind, double t_start, double t_end, int int
   c->thermo_kind = kind; c->t_start = t_start; c->t_end = t_end; c->thermo_interval = interval;
   c->thermo_frac = frac; c->seed = seed;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 

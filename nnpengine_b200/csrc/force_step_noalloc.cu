@@ -65,5 +65,6 @@ extern "C" int nnpe_force_step_noalloc(nnpe_ctx* c, const float* x_host, float* 
     stage = g_stage_addr[c->device];
   }
   if (!stage) return nnpe_fail(c, NNPE_EARG, "nnpe_force_step_noalloc: the static staging was not resolved by nnpe_setup");
-  return force_step_staged(c, x_host, f_host, erg, virial, stage, stage + 3 * kStageMaxAtoms);
+  // eager launches: instantiating a graph could allocate, which this entry point promises not to do
+  return force_step_staged(c, x_host, f_host, erg, virial, stage, stage + 3 * kStageMaxAtoms, false);
 }

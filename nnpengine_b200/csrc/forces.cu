@@ -549,26 +549,72 @@ int refuse_if_poisoned(nnpe_ctx* c) {
   return 0;
 }
 
+// The device part of the host-owned force step, between the positions' copy in and the forces' copy
+// out: positions into the sorted state, list check and (device-conditional) rebuild, images, forces,
+// optional energy reduction, forces gathered back into atom-id order.
+static int force_step_body(nnpe_ctx* c, bool ev, float* xstage, float* fstage) {
+  const int N = c->natom;
+  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(xstage, c->d_atom_id, c->d_xd, c->d_pos, N, (double)c->grid.bl, c->fp64_state);
+  if (int rc = check_valid_enqueue(c)) return rc;
+  if (int rc = rebuild_enqueue(c, true)) return rc;
+  if (int rc = ghost_update_enqueue(c, true)) return rc;
+  if (int rc = forces_enqueue(c, ev)) return rc;
+  if (ev)
+    if (int rc = energy_reduce_enqueue(c, 0)) return rc;
+  k_gather_forces<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_frc, c->d_atom_id, fstage, N);
+  NNPE_CHECK_LAUNCH(c);
+  return 0;
+}
+
+// The body runs as one CUDA graph launch (about thirty kernels, most of them tiny or exiting at once
+// when no rebuild is due, which a host would otherwise launch one by one at a few microseconds
+// each). The graph is captured on first use per (energies, staging) and dropped whenever the
+// context's step graphs are (any change of the set-up, tables, network or grids).
+static int force_step_launch(nnpe_ctx* c, bool ev, float* xstage, float* fstage) {
+  if (!c->fs_valid) {
+    for (auto& g : c->fs_graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->fs_valid = true;
+  }
+  const int v = ev ? 1 : 0;
+  if (c->fs_graph[v] && c->fs_xstage[v] != xstage) {
+    cudaGraphExecDestroy(c->fs_graph[v]);
+    c->fs_graph[v] = nullptr;
+  }
+  if (!c->fs_graph[v]) {
+    cudaGraph_t g;
+    NNPE_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = force_step_body(c, ev, xstage, fstage);
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return nnpe_fail(c, NNPE_ECUDA, std::string("force step capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&c->fs_graph[v], g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      c->fs_graph[v] = nullptr;
+      return nnpe_fail(c, NNPE_ECUDA, std::string("force step graph: ") + cudaGetErrorString(ei));
+    }
+    c->fs_xstage[v] = xstage;
+  }
+  NNPE_CUDA(c, cudaGraphLaunch(c->fs_graph[v], c->stream));
+  return 0;
+}
+
 int force_step_staged(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial, float* xstage,
-                      float* fstage) {
+                      float* fstage, bool graph) {
   if (int rc = refuse_if_poisoned(c)) return rc;
   const int N = c->natom;
   if (!c->first_step_done && !c->force_step_init) {
     k_qm_to_pos<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_qm, c->d_pos, N);
     c->force_step_init = true;
   }
-  NNPE_CUDA(c, cudaMemcpyAsync(xstage, x_host, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, c->stream));
-  k_scatter_positions<<<nblocks(N, 256), 256, 0, c->stream>>>(xstage, c->d_atom_id, c->d_xd, c->d_pos, N, (double)c->grid.bl, c->fp64_state);
-  if (int rc = check_valid_enqueue(c)) return rc;
-  if (int rc = rebuild_enqueue(c, true)) return rc;
-  if (int rc = ghost_update_enqueue(c, true)) return rc;
   const bool ev = erg || virial;
-  if (int rc = forces_enqueue(c, ev)) return rc;
-  if (ev) {
-    if (int rc = energy_reduce_enqueue(c, 0)) return rc;
-    NNPE_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
-  }
-  k_gather_forces<<<nblocks(N, 256), 256, 0, c->stream>>>(c->d_frc, c->d_atom_id, fstage, N);
+  NNPE_CUDA(c, cudaMemcpyAsync(xstage, x_host, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, c->stream));
+  if (int rc = graph ? force_step_launch(c, ev, xstage, fstage) : force_step_body(c, ev, xstage, fstage)) return rc;
+  if (ev) NNPE_CUDA(c, cudaMemcpyAsync(c->h_red, c->d_red, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaMemcpyAsync(f_host, fstage, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, c->stream));
   NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
   if (ev) {
@@ -586,7 +632,7 @@ extern "C" int nnpe_force_step(nnpe_ctx* c, const float* x_host, float* f_host, 
     NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_xstage, sizeof(float) * 3 * N));
     NNPE_CUDA(c, dev_malloc(c, (void**)&c->d_fstage, sizeof(float) * 3 * N));
   }
-  return force_step_staged(c, x_host, f_host, erg, virial, c->d_xstage, c->d_fstage);
+  return force_step_staged(c, x_host, f_host, erg, virial, c->d_xstage, c->d_fstage, true);
 }
 
 extern "C" int nnpe_compute_forces(nnpe_ctx* c, int ev, double* erg, double* virial) {

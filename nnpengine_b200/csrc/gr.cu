@@ -165,6 +165,7 @@ extern "C" int nnpe_gr_setup(nnpe_ctx* c, int nbin_inner, int nq, double qmax, i
   NNPE_CUDA(c, cudaFuncSetAttribute(k_gr_tally<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   NNPE_CUDA(c, cudaFuncSetAttribute(k_gr_tally<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 

@@ -242,6 +242,7 @@ static int prepare_run(nnpe_ctx* c, int max_log) {
     for (auto& g : c->graph_exec)
       if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     c->graph_valid = false;
+    c->fs_valid = false;
   }
   NNPE_CUDA(c, cudaMemsetAsync(c->d_ctrl + CTRL_NLOG, 0, sizeof(int), c->stream));
   if (!c->first_step_done) {
@@ -379,6 +380,7 @@ extern "C" int nnpe_set_total_steps(nnpe_ctx* c, int total) {
   if (!c) return NNPE_EARG;
   c->total_steps_hint = total;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 

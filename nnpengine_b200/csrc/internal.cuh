@@ -154,6 +154,10 @@ struct nnpe_ctx {
   // CUDA graphs of the step variants
   cudaGraphExec_t graph_exec[16] = {};
   bool graph_valid = false;
+  // CUDA graphs of the host-owned force step (without / with energies), keyed by their staging
+  float* fs_xstage[2] = {};
+  cudaGraphExec_t fs_graph[2] = {};
+  bool fs_valid = false;
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -222,9 +226,10 @@ int alloc_state(nnpe_ctx* c);
 int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
 int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6 = true);
 // The host-positions force step (nnpe_force_step) with its staging buffers given by the caller:
-// xstage and fstage hold at least 3 * natom floats each on the context's device.
+// xstage and fstage hold at least 3 * natom floats each on the context's device. graph: launch the
+// device part as the context's cached CUDA graph (else kernel by kernel).
 int force_step_staged(nnpe_ctx* c, const float* x_host, float* f_host, double* erg, double* virial, float* xstage,
-                      float* fstage);
+                      float* fstage, bool graph);
 // Resolves the device address of the allocation-free step's static staging on c's device (loading
 // the module that holds it); nnpe_setup calls it so that later steps load and reserve nothing.
 int noalloc_stage_prepare(nnpe_ctx* c);

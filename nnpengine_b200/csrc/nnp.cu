@@ -65,6 +65,7 @@ int nnpe_nnp_enable(nnpe_ctx* c, int on) {
   if (!c || !c->nnp) return nnpe_fail(c, NNPE_EARG, "nnpe_nnp_enable: no network");
   c->nnp->enabled = on != 0;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
@@ -200,6 +201,7 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
     if (int r2 = nnp_set_smem_attrs(c, smem_desc, smem_force)) return r2;
   }
   c->graph_valid = false;
+  c->fs_valid = false;
   return nnp_tc_setup(c);
 }
 
@@ -208,6 +210,7 @@ int nnpe_nnp_precision(nnpe_ctx* c, int bf16) {
   if (bf16 && c->nnp->kind != 1) return nnpe_fail(c, NNPE_EARG, "BF16 tensor-core path is for the embedding network");
   c->nnp->bf16 = bf16 != 0;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 

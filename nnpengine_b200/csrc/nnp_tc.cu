@@ -1069,6 +1069,7 @@ int nnp_tc_autotune(nnpe_ctx* c, int reps, bool use_cache, int* grid_desc, int* 
       t->grid_desc = std::min(it->second.first, c->natom);
       t->grid_force = std::min(it->second.second, c->natom);
       c->graph_valid = false;
+      c->fs_valid = false;
       if (grid_desc) *grid_desc = t->grid_desc;
       if (grid_force) *grid_force = t->grid_force;
       return NNPE_OK;
@@ -1114,6 +1115,7 @@ int nnp_tc_autotune(nnpe_ctx* c, int reps, bool use_cache, int* grid_desc, int* 
   }
   t->grid_force = best_f;
   c->graph_valid = false;
+  c->fs_valid = false;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = {best_d, best_f};
@@ -1130,6 +1132,7 @@ int nnp_tc_set_grids(nnpe_ctx* c, int grid_desc, int grid_force) {
   t->grid_desc = grid_desc > 0 ? std::min(grid_desc, std::max(c->natom, 1)) : 0;
   t->grid_force = grid_force > 0 ? std::min(grid_force, std::max(c->natom, 1)) : 0;
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 

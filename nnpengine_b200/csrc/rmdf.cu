@@ -238,6 +238,7 @@ extern "C" int nnpe_rmdf_set(nnpe_ctx* c, int n_sq, const double* sqex, const do
   double zero5 = 0;
   NNPE_CUDA(c, cudaMemcpy(c->d_red + 4, &zero5, sizeof(double), cudaMemcpyHostToDevice));
   c->graph_valid = false;
+  c->fs_valid = false;
   return NNPE_OK;
 }
 
