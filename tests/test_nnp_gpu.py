@@ -215,3 +215,36 @@ def test_autotuned_grids_same_bits_for_same_grid_and_bf16_bar_across_grids():
     assert cases.rel_rms(f_tuned, r["f"]) < 1e-2
     for e in (tuned, fixed, default):
         assert e.device_errors() == 0
+
+
+@pytest.mark.parametrize("rho", [0.003, 0.2])
+def test_embed_nnp_fp32_sparse_and_dense_pair_counts(rho):
+    """The FP32 kernels take each atom's pairs species by species in ballot-compacted chunks of up to
+    32 (the force kernel in groups of 16): a dilute mixture (most atoms without a pair inside 6 A)
+    and a dense one (about 180 pairs per atom, several chunks per species) both match the FP64
+    oracle at the plain form's bars, and atoms without pairs get a zero descriptor."""
+    from nnpengine_b200 import systems as S
+    s = S.lj_mixture(600, rho, 0.6, seed=5)
+    m = NM.embed_model()
+    e = Engine(0)
+    e.set_system(s)
+    e.set_velocities(np.zeros_like(s.v))
+    e.setup(6.0, 2.0, 6.0, 2048)
+    e.pair_enable(False)
+    e.nnp_set(m, 6.0, 750)
+    e.nnp_precision(False)
+    e.list_build()
+    erg, _ = e.compute_forces(True)
+    assert e.device_errors() == 0
+    r, G, dG, ea = _bf16_vs_fp64(s, m, e)
+    lone = np.all(r["G"] == 0, axis=1)
+    if rho < 0.01:
+        assert lone.sum() > 100
+    else:
+        assert not lone.any()
+    assert np.all(G[lone] == 0)
+    assert cases.rel_rms(G, r["G"]) < 1e-5
+    assert cases.rel_rms(e.forces(), r["f"]) < 1e-5
+    assert abs(ea.sum() - r["e_net"]) < 1e-5 * abs(r["e_net"])
+    e.compute_forces(True)   # deterministic
+    np.testing.assert_array_equal(e.nnp_get()[0], G)
