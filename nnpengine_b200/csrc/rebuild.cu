@@ -43,39 +43,57 @@ __global__ void k_refold_bin(double4* __restrict__ xd, int* __restrict__ ctmp, i
 }
 
 // Exclusive scan of n counts by one block: start[k] = offset + sum(in[<k]), end[k] = start[k] + in[k].
-__global__ void k_scan(const int* __restrict__ in, int n, int* __restrict__ start, int* __restrict__ end, int offset,
-                       int* total, const int* ctrl, bool cond) {
+__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ in, int n, int* __restrict__ start,
+                                               int* __restrict__ end, int offset, int* total, const int* ctrl, bool cond) {
   if (skip(ctrl, cond)) return;
+  // One block of 1024 threads over segments of 8192 values: each segment is loaded into shared
+  // memory with coalesced reads, every thread scans 8 consecutive values there, the 1024 thread
+  // totals are scanned with warp shuffles, and the results go back out with coalesced writes.
+  constexpr int kPer = 8, kSeg = 1024 * kPer;
+  __shared__ __align__(16) int buf[kSeg];
   __shared__ int warp_sums[32];
-  const int t = threadIdx.x, T = blockDim.x;
-  const int chunk = (n + T - 1) / T;
-  const int k0 = min(n, t * chunk), k1 = min(n, k0 + chunk);
-  int local = 0;
-  for (int k = k0; k < k1; ++k) local += in[k];
-  // block exclusive scan of `local`
-  int v = local;
-  for (int o = 1; o < 32; o <<= 1) {
-    int u = __shfl_up_sync(0xffffffffu, v, o);
-    if ((t & 31) >= o) v += u;
-  }
-  if ((t & 31) == 31) warp_sums[t >> 5] = v;
-  __syncthreads();
-  if (t < 32) {
-    int w = t < (T >> 5) ? warp_sums[t] : 0;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  int carry = offset;
+  for (int seg = 0; seg < n; seg += kSeg) {
+    const int m = min(kSeg, n - seg);
+    for (int k = t; k < kSeg; k += 1024) buf[k] = k < m ? in[seg + k] : 0;
+    __syncthreads();
+    int4* mine = reinterpret_cast<int4*>(buf + t * kPer);
+    const int4 a = mine[0], b = mine[1];
+    const int local = a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;
+    int v = local;   // inclusive scan over the warp
     for (int o = 1; o < 32; o <<= 1) {
-      int u = __shfl_up_sync(0xffffffffu, w, o);
-      if (t >= o) w += u;
+      const int u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
     }
-    warp_sums[t] = w;
+    if (lane == 31) warp_sums[w] = v;
+    __syncthreads();
+    if (w == 0) {
+      int x = warp_sums[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += u;
+      }
+      warp_sums[lane] = x;
+    }
+    __syncthreads();
+    int p0 = carry + v - local + (w ? warp_sums[w - 1] : 0);   // exclusive prefix of this thread's 8
+    const int seg_total = warp_sums[31];
+    int4 sa, sb;
+    sa.x = p0; p0 += a.x; sa.y = p0; p0 += a.y; sa.z = p0; p0 += a.z; sa.w = p0; p0 += a.w;
+    sb.x = p0; p0 += b.x; sb.y = p0; p0 += b.y; sb.z = p0; p0 += b.z; sb.w = p0;
+    mine[0] = sa;
+    mine[1] = sb;
+    __syncthreads();
+    for (int k = t; k < m; k += 1024) {
+      const int sv = buf[k];
+      start[seg + k] = sv;
+      if (end) end[seg + k] = sv + in[seg + k];
+    }
+    carry += seg_total;
+    __syncthreads();   // buf and warp_sums are reused by the next segment
   }
-  __syncthreads();
-  int prefix = v - local + ((t >> 5) ? warp_sums[(t >> 5) - 1] : 0) + offset;
-  for (int k = k0; k < k1; ++k) {
-    start[k] = prefix;
-    prefix += in[k];
-    if (end) end[k] = prefix;
-  }
-  if (t == T - 1 && total) *total = prefix;
+  if (t == 0 && total) *total = carry;
 }
 
 __global__ void k_scatter(const int* __restrict__ ctmp, const int* __restrict__ slot, const int* __restrict__ cstart,
