@@ -66,6 +66,11 @@ __device__ __forceinline__ uint32_t pack_bf2(float lo, float hi) {
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
+// (w0 u + b0, w1 u + b1) on the packed FP32 pipe, rounded to BF16 and packed.
+__device__ __forceinline__ uint32_t pack_fma2(float w0, float w1, float2 u2, float b0, float b1) {
+  const float2 v = __ffma2_rn(make_float2(w0, w1), u2, make_float2(b0, b1));
+  return pack_bf2(v.x, v.y);
+}
 // tanh of two packed BF16 values (one transcendental-unit operation for both).
 __device__ __forceinline__ uint32_t tanh_bf2(uint32_t x) {
   uint32_t y;
@@ -151,7 +156,7 @@ struct DescArgs {
   uint32_t* G2;                 // descriptor rows [N][256] BF16, two per word (the fitting kernel's operand)
   int* ctrl;
   int cap6, N, ntype, npos;
-  float rc, scale;
+  float rc, scale, r_rc;   // r_rc = 1/rc
 };
 
 struct TileSeg { int a, k0, na, nb; };
@@ -227,22 +232,26 @@ __device__ __forceinline__ DescRow desc_first_layer(const DescArgs& d, const Row
   r.valid = f.valid; r.cs = 0.f; r.tj = 0; r.s = 0; r.la = f.la;
   if (!f.valid) return r;
   const float dx = f.xi.x - f.xj.x, dy = f.xi.y - f.xj.y, dz = f.xi.z - f.xj.z;
-  const float rr = sqrtf(dx * dx + dy * dy + dz * dz);
-  const float cf = rr - d.rc, den = 1.f + cf * cf;
-  r.cs = d.scale * (1.f - 1.f / den);
+  // approximate square root and reciprocal (the hardware rsqrt / rcp units): a few ulp, far below
+  // the BF16 rounding of the operands they feed; cff = 1 - 1/(1+cf^2) = cf^2/(1+cf^2)
+  const float rsq = dx * dx + dy * dy + dz * dz;
+  const float rr = rsq * rsqrtf(rsq);
+  const float cf = rr - d.rc;
+  r.cs = d.scale * __fdividef(cf * cf, 1.f + cf * cf);
   r.s = f.ent >> 30;
   r.tj = (f.ent >> 27) & 7;
-  const float u = rr / d.rc;
+  const float u = rr * d.r_rc;
+  const float2 u2 = make_float2(u, u);
   const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
   const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
 #pragma unroll
   for (int g = 0; g < 4; ++g) {   // 8 units per 16-byte chunk, tanh on BF16 pairs (h is a BF16 operand)
     const float4 w0 = W1[2 * g], w1 = W1[2 * g + 1], b0 = B1[2 * g], b1 = B1[2 * g + 1];
     uint4 h;
-    h.x = tanh_bf2(pack_bf2(fmaf(w0.x, u, b0.x), fmaf(w0.y, u, b0.y)));
-    h.y = tanh_bf2(pack_bf2(fmaf(w0.z, u, b0.z), fmaf(w0.w, u, b0.w)));
-    h.z = tanh_bf2(pack_bf2(fmaf(w1.x, u, b1.x), fmaf(w1.y, u, b1.y)));
-    h.w = tanh_bf2(pack_bf2(fmaf(w1.z, u, b1.z), fmaf(w1.w, u, b1.w)));
+    h.x = tanh_bf2(pack_fma2(w0.x, w0.y, u2, b0.x, b0.y));
+    h.y = tanh_bf2(pack_fma2(w0.z, w0.w, u2, b0.z, b0.w));
+    h.z = tanh_bf2(pack_fma2(w1.x, w1.y, u2, b1.x, b1.y));
+    h.w = tanh_bf2(pack_fma2(w1.z, w1.w, u2, b1.z, b1.w));
     *reinterpret_cast<uint4*>(A + tc::kmajor_off(p, 32 * r.tj + 8 * g, kK64)) = h;
     *reinterpret_cast<uint4*>(A + tc::kmajor_off(p, 32 * (1 - r.tj) + 8 * g, kK64)) = make_uint4(0, 0, 0, 0);
   }
@@ -392,8 +401,10 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const float4 bb = b2[(c0 >> 2) + q];
-          y[2 * q] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q] + bb.x, z[4 * q + 1] + bb.y)), cs2);
-          y[2 * q + 1] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q + 2] + bb.z, z[4 * q + 3] + bb.w)), cs2);
+          const float2 zb0 = __fadd2_rn(make_float2(z[4 * q], z[4 * q + 1]), make_float2(bb.x, bb.y));
+          const float2 zb1 = __fadd2_rn(make_float2(z[4 * q + 2], z[4 * q + 3]), make_float2(bb.z, bb.w));
+          y[2 * q] = mul_bf2(tanh_bf2(pack_bf2(zb0.x, zb0.y)), cs2);
+          y[2 * q + 1] = mul_bf2(tanh_bf2(pack_bf2(zb1.x, zb1.y)), cs2);
         }
         if (p < NK) {   // rows past the tile's pairs are exact zeros (their Z may be anything)
 #pragma unroll
@@ -463,11 +474,11 @@ struct ForceArgs {
   unsigned long long* facc;   // [N][4]: force x, y, z and virial, fixed point (2^-32)
   int* ctrl;
   int cap6, N, ntype, npos;
-  float rc, scale;
+  float rc, scale, r_rc;   // r_rc = 1/rc
 };
 
 struct ForceRow {
-  float dx, dy, dz, r, rsq, cff, dcff;
+  float dx, dy, dz, rinv, rsq, cff, dcff;
   int s, tj, la, jo;
   bool valid;
 };
@@ -476,18 +487,22 @@ __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const 
                                                       unsigned char* AH, unsigned char* AV, int p, int half) {
   ForceRow r;
   r.valid = f.valid; r.la = f.la; r.s = 0; r.tj = 0; r.jo = 0;
-  r.dx = r.dy = r.dz = 0.f; r.r = 1.f; r.rsq = 1.f; r.cff = 0.f; r.dcff = 0.f;
+  r.dx = r.dy = r.dz = 0.f; r.rinv = 1.f; r.rsq = 1.f; r.cff = 0.f; r.dcff = 0.f;
   if (!f.valid) return r;
   r.dx = f.xi.x - f.xj.x; r.dy = f.xi.y - f.xj.y; r.dz = f.xi.z - f.xj.z;
   r.rsq = r.dx * r.dx + r.dy * r.dy + r.dz * r.dz;
-  r.r = sqrtf(r.rsq);
-  const float cf = r.r - a.rc, den = 1.f + cf * cf;
-  r.cff = 1.f - 1.f / den;
-  r.dcff = 2.f * cf / (den * den);
+  // approximate rsqrt / rcp (a few ulp, below the BF16 rounding of the operands they feed);
+  // cff = cf^2/(1+cf^2), dcff = 2 cf/(1+cf^2)^2
+  r.rinv = rsqrtf(r.rsq);
+  const float rr = r.rsq * r.rinv;
+  const float cf = rr - a.rc, rd = __fdividef(1.f, 1.f + cf * cf);
+  r.cff = cf * cf * rd;
+  r.dcff = 2.f * cf * rd * rd;
   r.s = f.ent >> 30;
   r.tj = (f.ent >> 27) & 7;
   r.jo = f.jo;
-  const float r_rc = 1.f / a.rc, u = r.r * r_rc;
+  const float u = rr * a.r_rc;
+  const float2 u2 = make_float2(u, u);
   const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
   const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
   const uint4* WR = reinterpret_cast<const uint4*>(sE + r.tj * kEmbStride4 + kWrOff);
@@ -499,10 +514,10 @@ __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const 
     // h on BF16 pairs (it is a BF16 operand), and V = (1 - h^2) w / rc from it on BF16 pairs: one
     // transcendental-unit operation per two units, the derivative without conversions
     uint4 h, v;
-    h.x = tanh_bf2(pack_bf2(fmaf(w0.x, u, b0.x), fmaf(w0.y, u, b0.y)));
-    h.y = tanh_bf2(pack_bf2(fmaf(w0.z, u, b0.z), fmaf(w0.w, u, b0.w)));
-    h.z = tanh_bf2(pack_bf2(fmaf(w1.x, u, b1.x), fmaf(w1.y, u, b1.y)));
-    h.w = tanh_bf2(pack_bf2(fmaf(w1.z, u, b1.z), fmaf(w1.w, u, b1.w)));
+    h.x = tanh_bf2(pack_fma2(w0.x, w0.y, u2, b0.x, b0.y));
+    h.y = tanh_bf2(pack_fma2(w0.z, w0.w, u2, b0.z, b0.w));
+    h.z = tanh_bf2(pack_fma2(w1.x, w1.y, u2, b1.x, b1.y));
+    h.w = tanh_bf2(pack_fma2(w1.z, w1.w, u2, b1.z, b1.w));
     const uint4 wr = WR[g];
     v.x = mul_bf2(fma_bf2(h.x ^ 0x80008000u, h.x, one2), wr.x);
     v.y = mul_bf2(fma_bf2(h.y ^ 0x80008000u, h.y, one2), wr.y);
@@ -556,7 +571,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   for (int k = t; k < 2 * 128; k += 256) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < a.ntype ? a.emb_small[k] : 0.f;
   for (int k = t; k < 2 * 16; k += 256) {
     const int sp = k >> 4, q = k & 15;
-    const float r_rc = 1.f / a.rc;
+    const float r_rc = a.r_rc;
     const float w0 = sp < a.ntype ? a.emb_small[sp * 128 + 2 * q] : 0.f, w1 = sp < a.ntype ? a.emb_small[sp * 128 + 2 * q + 1] : 0.f;
     reinterpret_cast<uint32_t*>(sE)[sp * kEmbStride4 + kWrOff + q] = pack_bf2(w0 * r_rc, w1 * r_rc);
   }
@@ -641,7 +656,9 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     if (32 * (w & 3) < nrows) {   // warp-uniform: the loads below are warp-collective
       const float* ag = sdG + 512 * b0 + row0.la * 256 + row0.s * 64 + 32 * half;
       const float* b2 = sE + row0.tj * kEmbStride4 + 64 + 32 * half;
-      float sy = 0.f, sk = 0.f;
+      // channel pairs on the packed FP32 pipe (two lanes of arithmetic per instruction)
+      float2 sy2 = make_float2(0.f, 0.f), sk2 = make_float2(0.f, 0.f);
+      const float2 one2f = make_float2(1.f, 1.f);
 #pragma unroll
       for (int c0 = 0; c0 < 32; c0 += 16) {
         float z[16], kap[16];
@@ -650,16 +667,19 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
         for (int q = 0; q < 16; q += 4) {
           const float4 a4 = *reinterpret_cast<const float4*>(ag + c0 + q);
           const float4 bb = *reinterpret_cast<const float4*>(b2 + c0 + q);
-          const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {bb.x, bb.y, bb.z, bb.w};
+          const float2 av[2] = {make_float2(a4.x, a4.y), make_float2(a4.z, a4.w)};
+          const float2 bv[2] = {make_float2(bb.x, bb.y), make_float2(bb.z, bb.w)};
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const float y = tanh_fast(z[q + e] + bv[e]);
-            sy = fmaf(av[e], y, sy);
-            sk = fmaf(av[e] * kap[q + e], fmaf(-y, y, 1.f), sk);
+          for (int e = 0; e < 2; ++e) {
+            const float2 zb = __fadd2_rn(make_float2(z[q + 2 * e], z[q + 2 * e + 1]), bv[e]);
+            const float2 y = make_float2(tanh_fast(zb.x), tanh_fast(zb.y));
+            sy2 = __ffma2_rn(av[e], y, sy2);
+            const float2 u = __ffma2_rn(make_float2(-y.x, -y.y), y, one2f);
+            sk2 = __ffma2_rn(__fmul2_rn(av[e], make_float2(kap[q + 2 * e], kap[q + 2 * e + 1])), u, sk2);
           }
         }
       }
-      if (row0.valid) part = a.scale * (row0.dcff * sy + row0.cff * sk);
+      if (row0.valid) part = a.scale * (row0.dcff * (sy2.x + sy2.y) + row0.cff * (sk2.x + sk2.y));
     }
     sAcc[half * kTile + p] = part;
     fetch_xj(dv, f2, true);
@@ -669,7 +689,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     {
       float gx = 0.f, gy = 0.f, gz = 0.f, vr = 0.f;
       if (row0.valid) {
-        const float fpair = -(sAcc[p] + sAcc[kTile + p]) / row0.r;
+        const float fpair = -(sAcc[p] + sAcc[kTile + p]) * row0.rinv;
         gx = row0.dx * fpair; gy = row0.dy * fpair; gz = row0.dz * fpair;
         if (EV) vr = fpair * row0.rsq;
       }
@@ -1000,6 +1020,7 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   dd.pos = c->d_pos; dd.list6 = m->d_list6; dd.n6 = m->d_n6; dd.gowner = c->d_gowner;
   dd.wdesc = t->d_wdesc64; dd.emb_small = t->d_emb_small; dd.G2 = reinterpret_cast<uint32_t*>(m->d_G); dd.ctrl = c->d_ctrl;
   dd.cap6 = m->cap6; dd.N = c->natom; dd.ntype = c->ntype; dd.npos = c->natom + c->Gcap; dd.rc = m->rc; dd.scale = m->scale;
+  dd.r_rc = 1.f / m->rc;
   const int gdesc = t->grid_desc > 0 ? t->grid_desc : std::max(1, std::min(c->natom, sms * t->ctas_desc));
   k_tc_desc2<<<gdesc, 128, kSmemDesc2, c->stream>>>(dd);
   m->g_bf16 = true;
@@ -1014,6 +1035,7 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   fa.pos = c->d_pos; fa.list6 = m->d_list6; fa.n6 = m->d_n6; fa.gowner = c->d_gowner; fa.wdesc = t->d_wdesc64;
   fa.emb_small = t->d_emb_small; fa.dG = m->d_dG; fa.facc = t->d_facc; fa.ctrl = c->d_ctrl;
   fa.cap6 = m->cap6; fa.N = c->natom; fa.ntype = c->ntype; fa.npos = c->natom + c->Gcap; fa.rc = m->rc; fa.scale = m->scale;
+  fa.r_rc = 1.f / m->rc;
   const int gforce = t->grid_force > 0 ? t->grid_force : std::max(1, std::min(c->natom, sms * t->ctas_force));
   const int gapply = (c->natom + 255) / 256;
   if (ev) {
