@@ -9,7 +9,8 @@
 //
 //  k_tc_desc2   first layer h1 = tanh(W1 u + b1) per pair into the A tile, block-diagonal over the
 //               neighbour species, so one MMA chain gives every row the second layer of its own
-//               net; epilogue y = scale cff tanh(z + b2) (BF16 pairs); the sum over pairs into G by
+//               net (b2 enters the same chain as a one-hot K slice); epilogue y = scale cff
+//               tanh(z + b2) (BF16 pairs); the sum over pairs into G by
 //               atom segment and special class is a second MMA with a one-hot A (no atomics); G is
 //               stored as BF16 rows, the fitting kernel's operand type.
 //  k_tc_fit     128 atoms of one species per tile (G rows fetched by cp.async straight into the
@@ -133,7 +134,7 @@ __device__ __forceinline__ void fix_add(unsigned long long* dst, float v) {
 //   (2) barrier, after which MMA 1 of tile t is complete,
 //   (3) MMA 1 of tile t+1 into TMEM[(t+1) % 2] (Z = H W2s, K = 64 block-diagonal over the neighbour
 //       species; b2 is added in the epilogue),
-//   (4) epilogue of tile t: y = scale cff tanh(z + b2) -> Y (BF16, MN-major) over A[t % 2], and the
+//   (4) epilogue of tile t: y = scale cff tanh(z) -> Y (BF16, MN-major) over A[t % 2], and the
 //       one-hot S of the (la, s) rows,
 //   (5) barrier; MMA 2 of tile t: TMEM[t % 2] = S Y.
 // MMA 1 of tile t+1 runs during the epilogue of tile t and MMA 2 of tile t during the next
@@ -144,14 +145,29 @@ constexpr int kK64 = 64;
 constexpr int kEmbStride4 = 148;   // 16-byte aligned rows of the per-species constants: W1[32] b1[32] b2[64], 4 unused, WR[16]
 constexpr int kWrOff = 132;        // WR: w/rc of the first layer as BF16 pairs (the force kernel's r-derivative)
 constexpr int kDescStages = 2;
-constexpr int kSmemDesc2 = 64 * kK64 * 2 + kDescStages * kTile * kK64 * 2 + 8 * kTile * 2 + 2 * kEmbStride4 * 4 + 256 * 4;
+// The second layer's bias b2 enters MMA 1 as a fifth K=16 slice: A = the row's one-hot species
+// (column tj of a [128 x 16] tile whose columns 8..15 stay zero), B = b2 of each species (BF16), so
+// Z = H W2 + b2 leaves TMEM with the bias already added.
+constexpr int kWImg = 64 * kK64 * 2;            // B of MMA 1: [W2_0; W2_1], N = 64 x K = 64
+constexpr int kWBiasImg = 64 * 16 * 2;          // B of the bias slice: N = 64 x K = 16, column s = b2 of species s
+constexpr int kBiasA = kTile * 16 * 2;          // A of the bias slice, one per operand stage
+__device__ __forceinline__ uint32_t bias_a_off(int p) { return tc::kmajor_off(p, 0, 16); }
+// one-hot row chunk (k = 0..7) of species tj in BF16
+__device__ __forceinline__ uint4 onehot8(int tj) {
+  uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) w[k] = (tj == 2 * k ? 0x3F80u : 0u) | (tj == 2 * k + 1 ? 0x3F800000u : 0u);
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+constexpr int kSmemDesc2 = kWImg + kWBiasImg + kDescStages * kTile * kK64 * 2 + 8 * kTile * 2 + kDescStages * kBiasA +
+                           2 * kEmbStride4 * 4 + 256 * 4;
 
 struct DescArgs {
   const float4* pos;
   const uint32_t* list6;
   const int* n6;
   const int* gowner;
-  const unsigned char* wdesc;   // B of MMA 1: N = 64 channels x K = 64, [W2_0; W2_1]
+  const unsigned char* wdesc;   // B of MMA 1: N = 64 channels x K = 64, [W2_0; W2_1]; then the bias slice's B
   const float* emb_small;       // per species W1[32] b1[32] b2[64] (stride 128)
   uint32_t* G2;                 // descriptor rows [N][256] BF16, two per word (the fitting kernel's operand)
   int* ctrl;
@@ -227,7 +243,7 @@ struct DescRow {
 // First layer of one row into A (block of species tj, zeros in the other block); returns the
 // row's epilogue data.
 __device__ __forceinline__ DescRow desc_first_layer(const DescArgs& d, const RowFetch& f, const float* sE,
-                                                    unsigned char* A, int p) {
+                                                    unsigned char* A, unsigned char* AB, int p) {
   DescRow r;
   r.valid = f.valid; r.cs = 0.f; r.tj = 0; r.s = 0; r.la = f.la;
   if (!f.valid) return r;
@@ -242,6 +258,7 @@ __device__ __forceinline__ DescRow desc_first_layer(const DescArgs& d, const Row
   r.tj = (f.ent >> 27) & 7;
   const float u = rr * d.r_rc;
   const float2 u2 = make_float2(u, u);
+  *reinterpret_cast<uint4*>(AB + bias_a_off(p)) = onehot8(r.tj);
   const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
   const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
 #pragma unroll
@@ -294,10 +311,11 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   __shared__ uint64_t bar_z[2], bar_g;
   __shared__ uint32_t tmem_base;
   __shared__ int s_range[2];
-  unsigned char* sW = sm;                                       // B of MMA 1 (64 x 64)
-  unsigned char* sA = sW + 64 * kK64 * 2;                       // 3 x [128 x 64]: H of MMA 1, then Y of MMA 2
+  unsigned char* sW = sm;                                       // B of MMA 1 (64 x 64), then the bias slice's B
+  unsigned char* sA = sW + kWImg + kWBiasImg;                   // 2 x [128 x 64]: H of MMA 1, then Y of MMA 2
   unsigned char* sS = sA + kDescStages * kTile * kK64 * 2;      // A of MMA 2 (8 x 128)
-  float* sE = reinterpret_cast<float*>(sS + 8 * kTile * 2);     // per species W1 b1 b2 (stride 132)
+  unsigned char* sAB = sS + 8 * kTile * 2;                      // 2 x [128 x 16]: A of the bias slice
+  float* sE = reinterpret_cast<float*>(sAB + kDescStages * kBiasA);   // per species W1 b1 b2 (stride 148)
   float* sCarry = sE + 2 * kEmbStride4;                         // partial G of a segment cut by a tile end
   const int t = threadIdx.x, w = t >> 5, lane = t & 31, p = t;
   if (w == 0) tc::tmem_alloc(&tmem_base, 128);
@@ -311,7 +329,8 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
     s_range[0] = r[0];
     s_range[1] = r[1];
   }
-  copy_image(sW, d.wdesc, 64 * kK64 * 2, t, 128);
+  copy_image(sW, d.wdesc, kWImg + kWBiasImg, t, 128);
+  for (int k = t; k < kDescStages * kBiasA / 16; k += 128) reinterpret_cast<uint4*>(sAB)[k] = make_uint4(0, 0, 0, 0);
   for (int k = t; k < 2 * 128; k += 128) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < d.ntype ? d.emb_small[k] : 0.f;
   tc::fence_async_smem();
   tc::fence_before();
@@ -319,7 +338,7 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   tc::fence_after();
   const uint32_t tmem = tmem_base;
   const uint32_t lane_off = (uint32_t)(w * 32) << 16;
-  const uint32_t aW = tc::smem_u32(sW), aS = tc::smem_u32(sS);
+  const uint32_t aW = tc::smem_u32(sW), aS = tc::smem_u32(sS), aWB = aW + kWImg, aAB = tc::smem_u32(sAB);
   const int i1 = s_range[1];
   int ca = s_range[0], ck0 = 0;
   uint32_t ph_z[2] = {0, 0}, ph_g = 0;
@@ -333,7 +352,7 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   fetch_xj(d, f0);
   bool have1 = have0 && next_tile(d, ca, ck0, i1, seg1, t);
   fetch_entry(d, seg1, have1, p, f1);
-  DescRow row0 = desc_first_layer(d, f0, sE, sA, p);
+  DescRow row0 = desc_first_layer(d, f0, sE, sA, sAB, p);
   fetch_xj(d, f1);
   tc::fence_async_smem();
   tc::fence_before();
@@ -342,6 +361,7 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   if (have0 && t == 0) {
     const uint32_t id = tc::idesc_bf16(128, 64);
     for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(tc::smem_u32(sA), kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+    tc::mma_bf16(tmem, tc::tile_desc(aAB, 16, 0), tc::tile_desc(aWB, 16, 0), id, 1);
     tc::mma_commit(&bar_z[0]);
   }
   bool havep = false;
@@ -362,7 +382,7 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
     bool have2 = false;
     seg2 = TileSeg{0, 0, 0, 0};
     if (have1) {
-      row1 = desc_first_layer(d, f1, sE, A1, p);
+      row1 = desc_first_layer(d, f1, sE, A1, sAB + b1 * kBiasA, p);
       have2 = next_tile(d, ca, ck0, i1, seg2, t);
     }
     fetch_entry(d, seg2, have2, p, f2);
@@ -385,12 +405,12 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
       const uint32_t id = tc::idesc_bf16(128, 64);
       const uint32_t aA = tc::smem_u32(A1);
       for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem + 64 * b1, tc::tile_desc(aA, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+      tc::mma_bf16(tmem + 64 * b1, tc::tile_desc(aAB + b1 * kBiasA, 16, 0), tc::tile_desc(aWB, 16, 0), id, 1);
       tc::mma_commit(&bar_z[b1]);
     }
-    // (4) epilogue of tile it: y = scale cff tanh(z + b2), on BF16 pairs (Y is a BF16 operand)
+    // (4) epilogue of tile it: y = scale cff tanh(z) (z includes b2), on BF16 pairs (Y is a BF16 operand)
     const int nrows = seg0.na + seg0.nb, NK = (nrows + 15) & ~15;
     if (32 * w < NK) {   // warp-uniform
-      const float4* b2 = reinterpret_cast<const float4*>(sE + row0.tj * kEmbStride4 + 64);
       const float csv = row0.valid ? row0.cs : 0.f;
       const uint32_t cs2 = pack_bf2(csv, csv);
 #pragma unroll
@@ -400,11 +420,8 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
         uint32_t y[16];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const float4 bb = b2[(c0 >> 2) + q];
-          const float2 zb0 = __fadd2_rn(make_float2(z[4 * q], z[4 * q + 1]), make_float2(bb.x, bb.y));
-          const float2 zb1 = __fadd2_rn(make_float2(z[4 * q + 2], z[4 * q + 3]), make_float2(bb.z, bb.w));
-          y[2 * q] = mul_bf2(tanh_bf2(pack_bf2(zb0.x, zb0.y)), cs2);
-          y[2 * q + 1] = mul_bf2(tanh_bf2(pack_bf2(zb1.x, zb1.y)), cs2);
+          y[2 * q] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q], z[4 * q + 1])), cs2);
+          y[2 * q + 1] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q + 2], z[4 * q + 3])), cs2);
         }
         if (p < NK) {   // rows past the tile's pairs are exact zeros (their Z may be anything)
 #pragma unroll
@@ -458,10 +475,11 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
 //   (2) barrier, after which MMA of tile t is complete,
 //   (3) MMA of tile t+1: Z = H W2s and K = V W2s into TMEM stage (t+1) % 2 (128 columns),
 //   (4) epilogue of tile t: each half's share of T = scale (dcff sum_c a_c y_c + cff sum_c a_c
-//       kappa_c (1 - y_c^2)), y = tanh(z + b2), a = dE/dG_i[s*64 + c],
+//       kappa_c (1 - y_c^2)), y = tanh(z + b2) (b2 added by the H MMA's bias slice), a = dE/dG_i[s*64 + c],
 //   (5) barrier; half 0: fpair = -T/r applied to j's owner (64-bit fixed-point atomics) and summed
 //       per atom segment over each warp (one atomic per segment and warp) for i; the virial the same.
-constexpr int kSmemForce2 = 64 * kK64 * 2 + 2 * 2 * kTile * kK64 * 2 + 2 * 2 * 256 * 4 + 2 * kEmbStride4 * 4 + 2 * kTile * 4;
+constexpr int kSmemForce2 = kWImg + kWBiasImg + 2 * 2 * kTile * kK64 * 2 + 2 * kBiasA + 2 * 2 * 256 * 4 + 2 * kEmbStride4 * 4 +
+                            2 * kTile * 4;
 
 struct ForceArgs {
   const float4* pos;
@@ -484,7 +502,8 @@ struct ForceRow {
 };
 
 __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const RowFetch& f, const float* sE,
-                                                      unsigned char* AH, unsigned char* AV, int p, int half) {
+                                                      unsigned char* AH, unsigned char* AV, unsigned char* AB, int p,
+                                                      int half) {
   ForceRow r;
   r.valid = f.valid; r.la = f.la; r.s = 0; r.tj = 0; r.jo = 0;
   r.dx = r.dy = r.dz = 0.f; r.rinv = 1.f; r.rsq = 1.f; r.cff = 0.f; r.dcff = 0.f;
@@ -503,6 +522,7 @@ __device__ __forceinline__ ForceRow force_first_layer(const ForceArgs& a, const 
   r.jo = f.jo;
   const float u = rr * a.r_rc;
   const float2 u2 = make_float2(u, u);
+  if (half == 0) *reinterpret_cast<uint4*>(AB + bias_a_off(p)) = onehot8(r.tj);   // b2 enters the H MMA only
   const float4* W1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4);
   const float4* B1 = reinterpret_cast<const float4*>(sE + r.tj * kEmbStride4 + 32);
   const uint4* WR = reinterpret_cast<const uint4*>(sE + r.tj * kEmbStride4 + kWrOff);
@@ -556,9 +576,10 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_base;
-  unsigned char* sW = sm;                                          // 64 x 64
-  unsigned char* sAH = sW + 64 * kK64 * 2;                         // 2 stages x [H | V], 32 KB each
-  float* sdG = reinterpret_cast<float*>(sAH + 2 * 2 * kTile * kK64 * 2);   // 2 stages x [2][256]
+  unsigned char* sW = sm;                                          // 64 x 64, then the bias slice's B
+  unsigned char* sAH = sW + kWImg + kWBiasImg;                     // 2 stages x [H | V], 32 KB each
+  unsigned char* sAB = sAH + 2 * 2 * kTile * kK64 * 2;             // 2 stages x [128 x 16]: A of the bias slice
+  float* sdG = reinterpret_cast<float*>(sAB + 2 * kBiasA);         // 2 stages x [2][256]
   float* sE = sdG + 2 * 512;
   float* sAcc = sE + 2 * kEmbStride4;                              // [2][128] per-half partial T
   const int t = threadIdx.x, w = t >> 5, lane = t & 31, p = t & 127, half = t >> 7;
@@ -567,7 +588,8 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     tc::mbar_init(&bar[0], 1);
     tc::mbar_init(&bar[1], 1);
   }
-  copy_image(sW, a.wdesc, 64 * kK64 * 2, t, 256);
+  copy_image(sW, a.wdesc, kWImg + kWBiasImg, t, 256);
+  for (int k = t; k < 2 * kBiasA / 16; k += 256) reinterpret_cast<uint4*>(sAB)[k] = make_uint4(0, 0, 0, 0);
   for (int k = t; k < 2 * 128; k += 256) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < a.ntype ? a.emb_small[k] : 0.f;
   for (int k = t; k < 2 * 16; k += 256) {
     const int sp = k >> 4, q = k & 15;
@@ -581,7 +603,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   tc::fence_after();
   const uint32_t tmem = tmem_base;
   const uint32_t lane_off = (uint32_t)((w & 3) * 32) << 16;
-  const uint32_t aW = tc::smem_u32(sW);
+  const uint32_t aW = tc::smem_u32(sW), aWB = aW + kWImg, aAB = tc::smem_u32(sAB);
   const int i0 = (int)((long long)a.N * blockIdx.x / gridDim.x), i1 = (int)((long long)a.N * (blockIdx.x + 1) / gridDim.x);
   int ca = i0, ck0 = 0;
   uint32_t ph[2] = {0, 0};
@@ -598,7 +620,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   bool have1 = have0 && next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg1, t, 256);
   fetch_entry(dv, seg1, have1, p, f1);
   float2 g1 = fetch_tile_dG(a, seg1, have1, t);
-  ForceRow row0 = force_first_layer(a, f0, sE, sAH, sAH + kTile * kK64 * 2, p, half);
+  ForceRow row0 = force_first_layer(a, f0, sE, sAH, sAH + kTile * kK64 * 2, sAB, p, half);
   if (have0) store_tile_dG(g0, sdG, t);
   fetch_xj(dv, f1, true);
   tc::fence_async_smem();
@@ -609,6 +631,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     const uint32_t id = tc::idesc_bf16(128, 64);
     const uint32_t aH = tc::smem_u32(sAH), aV = aH + kTile * kK64 * 2;
     for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem, tc::tile_desc(aH, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+    tc::mma_bf16(tmem, tc::tile_desc(aAB, 16, 0), tc::tile_desc(aWB, 16, 0), id, 1);
     for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(tmem + 64, tc::tile_desc(aV, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
     tc::mma_commit(&bar[0]);
   }
@@ -621,7 +644,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     seg2 = TileSeg{0, 0, 0, 0};
     float2 g2 = make_float2(0.f, 0.f);
     if (have1) {
-      row1 = force_first_layer(a, f1, sE, AH1, AH1 + kTile * kK64 * 2, p, half);
+      row1 = force_first_layer(a, f1, sE, AH1, AH1 + kTile * kK64 * 2, sAB + b1 * kBiasA, p, half);
       store_tile_dG(g1, sdG + 512 * b1, t);
       have2 = next_tile_n6(a.n6, nullptr, ca, ck0, i1, seg2, t, 256);
     }
@@ -647,6 +670,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
       const uint32_t aH = tc::smem_u32(AH1), aV = aH + kTile * kK64 * 2;
       const uint32_t td = tmem + 128 * b1;
       for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(td, tc::tile_desc(aH, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
+      tc::mma_bf16(td, tc::tile_desc(aAB + b1 * kBiasA, 16, 0), tc::tile_desc(aWB, 16, 0), id, 1);
       for (int kk = 0; kk < kK64 / 16; ++kk) tc::mma_bf16(td + 64, tc::tile_desc(aV, kK64, kk), tc::tile_desc(aW, kK64, kk), id, kk > 0);
       tc::mma_commit(&bar[b1]);
     }
@@ -655,7 +679,6 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
     float part = 0.f;
     if (32 * (w & 3) < nrows) {   // warp-uniform: the loads below are warp-collective
       const float* ag = sdG + 512 * b0 + row0.la * 256 + row0.s * 64 + 32 * half;
-      const float* b2 = sE + row0.tj * kEmbStride4 + 64 + 32 * half;
       // channel pairs on the packed FP32 pipe (two lanes of arithmetic per instruction)
       float2 sy2 = make_float2(0.f, 0.f), sk2 = make_float2(0.f, 0.f);
       const float2 one2f = make_float2(1.f, 1.f);
@@ -666,13 +689,10 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
 #pragma unroll
         for (int q = 0; q < 16; q += 4) {
           const float4 a4 = *reinterpret_cast<const float4*>(ag + c0 + q);
-          const float4 bb = *reinterpret_cast<const float4*>(b2 + c0 + q);
           const float2 av[2] = {make_float2(a4.x, a4.y), make_float2(a4.z, a4.w)};
-          const float2 bv[2] = {make_float2(bb.x, bb.y), make_float2(bb.z, bb.w)};
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
-            const float2 zb = __fadd2_rn(make_float2(z[q + 2 * e], z[q + 2 * e + 1]), bv[e]);
-            const float2 y = make_float2(tanh_fast(zb.x), tanh_fast(zb.y));
+            const float2 y = make_float2(tanh_fast(z[q + 2 * e]), tanh_fast(z[q + 2 * e + 1]));   // z includes b2
             sy2 = __ffma2_rn(av[e], y, sy2);
             const float2 u = __ffma2_rn(make_float2(-y.x, -y.y), y, one2f);
             sk2 = __ffma2_rn(__fmul2_rn(av[e], make_float2(kap[q + 2 * e], kap[q + 2 * e + 1])), u, sk2);
@@ -957,8 +977,10 @@ int nnp_tc_setup(nnpe_ctx* c) {
   const int T = c->ntype;
   const size_t eb = 32 + 32 + 32 * 64 + 64;
   const float* E = m->h_embw.data();
-  std::vector<uint16_t> wdesc64((size_t)64 * kK64);
+  std::vector<uint16_t> wdesc64((size_t)(kWImg + kWBiasImg) / 2);
   put_image(wdesc64, 0, 64, kK64, [&](int n, int k) { return k / 32 < T ? E[eb * (k / 32) + 64 + (k % 32) * 64 + n] : 0.f; });
+  // the bias slice's B: column s = b2 of species s (the A slice is the row's one-hot species)
+  put_image(wdesc64, kWImg / 2, 64, 16, [&](int n, int k) { return k < T ? E[eb * k + 64 + 32 * 64 + n] : 0.f; });
   std::vector<float> emb_small((size_t)T * 128);
   for (int s = 0; s < T; ++s)
     for (int q = 0; q < 32; ++q) {
