@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
   __shared__ int s_range[2];
   unsigned char* sW = sm;                                       // B of MMA 1 (64 x 64), then the bias slice's B
   unsigned char* sA = sW + kWImg + kWBiasImg;                   // 2 x [128 x 64]: H of MMA 1, then Y of MMA 2
-  unsigned char* sS = sA + kDescStages * kTile * kK64 * 2;      // A of MMA 2 (8 x 128)
+  unsigned char* sS = sA + kDescStages * kTile * kK64 * 2;      // A of MMA 2 (8 x 128, MN-major)
   unsigned char* sAB = sS + 8 * kTile * 2;                      // 2 x [128 x 16]: A of the bias slice
   float* sE = reinterpret_cast<float*>(sAB + kDescStages * kBiasA);   // per species W1 b1 b2 (stride 148)
   float* sCarry = sE + 2 * kEmbStride4;                         // partial G of a segment cut by a tile end
@@ -330,6 +330,8 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
     s_range[1] = r[1];
   }
   copy_image(sW, d.wdesc, kWImg + kWBiasImg, t, 128);
+  // operand stages and bias slices start zeroed (rows past a tile's pairs must read finite values)
+  for (int k = t; k < kDescStages * kTile * kK64 * 2 / 16; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
   for (int k = t; k < kDescStages * kBiasA / 16; k += 128) reinterpret_cast<uint4*>(sAB)[k] = make_uint4(0, 0, 0, 0);
   for (int k = t; k < 2 * 128; k += 128) sE[(k >> 7) * kEmbStride4 + (k & 127)] = (k >> 7) < d.ntype ? d.emb_small[k] : 0.f;
   tc::fence_async_smem();
@@ -423,20 +425,18 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
           y[2 * q] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q], z[4 * q + 1])), cs2);
           y[2 * q + 1] = mul_bf2(tanh_bf2(pack_bf2(z[4 * q + 2], z[4 * q + 3])), cs2);
         }
-        if (p < NK) {   // rows past the tile's pairs are exact zeros (their Z may be anything)
+        // Rows past the tile's pairs carry y = 0 (cs = 0) and a zero S column. Their Z is finite:
+        // the operand stages start zeroed and afterwards hold earlier tiles' first layers, so
+        // 0 x Y adds exact zeros to G.
+        if (p < NK) {
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            *reinterpret_cast<uint4*>(A0 + tc::mnmajor_off(c0 + 8 * q, p, 64)) =
-                row0.valid ? make_uint4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]) : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(A0 + tc::mnmajor_off(c0 + 8 * q, p, 64)) = make_uint4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
         }
       }
-      if (p < NK) {
-        const int m = 4 * row0.la + row0.s;
-        const uint16_t one = 0x3F80u;
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          *reinterpret_cast<uint16_t*>(sS + tc::kmajor_off(c, p, kTile)) = (row0.valid && m == c) ? one : (uint16_t)0;
-      }
+      // S is held MN-major (row p of the pair dimension = 8 contiguous classes (la, s)): one 16-byte
+      // one-hot per row
+      if (p < NK) *reinterpret_cast<uint4*>(sS + 16 * p) = onehot8(row0.valid ? 4 * row0.la + row0.s : 8);
     }
     fetch_xj(d, f2);
     // (5) MMA 2 of tile it
@@ -445,10 +445,10 @@ __global__ void __launch_bounds__(128, 4) k_tc_desc2(DescArgs d) {
     __syncthreads();
     tc::fence_after();
     if (t == 0) {
-      const uint32_t id = tc::idesc_bf16(128, 64, true);
+      const uint32_t id = tc::idesc_bf16(128, 64, true, true);
       const uint32_t aY = tc::smem_u32(A0);
       for (int kk = 0; kk < NK / 16; ++kk)
-        tc::mma_bf16(tmem + 64 * b0, tc::tile_desc_bcast(aS, kTile, kk), tc::tile_desc_mn(aY, 64, kk), id, kk > 0);
+        tc::mma_bf16(tmem + 64 * b0, tc::tile_desc_bcast_mn(aS, kk), tc::tile_desc_mn(aY, 64, kk), id, kk > 0);
       tc::mma_commit(&bar_g);
     }
     segp = seg0; havep = true; last_buf = b0;

@@ -34,10 +34,10 @@ __device__ __forceinline__ uint64_t tile_desc(uint32_t saddr, int K, int kk) {
 }
 
 // instruction descriptor: kind::f16, A=B=BF16, D=F32, shape M x N; A and B K-major unless
-// b_mn (bit 16) selects an MN-major B operand
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool b_mn = false) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
+// b_mn (bit 16) / a_mn (bit 15) select an MN-major B / A operand
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool b_mn = false, bool a_mn = false) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // MN-major no-swizzle tile [N rows (MN) x K]: core matrix (n/8, k/8) holds 8 K-rows of 8 contiguous
@@ -51,6 +51,12 @@ __device__ __forceinline__ uint64_t tile_desc_mn(uint32_t saddr, int N, int kk) 
 // K-major descriptor whose 8-row groups all alias the first one (SBO = 0): an M x K operand whose
 // rows repeat with period 8, held in 8*K*2 bytes
 __device__ __forceinline__ uint64_t tile_desc_bcast(uint32_t saddr, int K, int kk) {
+  return sdesc(saddr + 256u * kk, 128u, 0u);
+}
+// MN-major counterpart: an M x K operand whose rows repeat with period 8, held as K rows of 8
+// contiguous M elements (element (m, k) at 16 k + 2 (m % 8)); K-adjacent core matrices 128 B apart
+// (LBO), MN-adjacent ones aliased (SBO = 0)
+__device__ __forceinline__ uint64_t tile_desc_bcast_mn(uint32_t saddr, int kk) {
   return sdesc(saddr + 256u * kk, 128u, 0u);
 }
 
