@@ -544,6 +544,8 @@ def main():
     ap.add_argument("--no-same-model", action="store_true", help="skip the GPU run of the reference's own model")
     ap.add_argument("--exact", action="store_true", help="pair forces in the reference's exact float sequence")
     ap.add_argument("--no-autotune", action="store_true", help="default grids for the tensor-core kernels")
+    ap.add_argument("--prune", type=float, default=None,
+                    help="dynamic list-pruning margin in A (0: off; default: the library's 0.5 A)")
     ap.add_argument("--cpu-steps", type=int, default=0, help="reference MD-loop sample: N and 2N steps (0: per workload)")
     ap.add_argument("--equil", type=int, default=5000)
     ap.add_argument("--serve-requests", type=int, default=256)
@@ -648,6 +650,8 @@ def main():
     s, table = build_system(wl, rank)
     e = make_engine(s, table, local, wl.get("nnp"))
     e.pair_exact(args.exact)
+    if args.prune is not None:
+        e.set_prune(args.prune)
     stream = torch.cuda.ExternalStream(e.lib.nnpe_stream(e.h))
     refine = wl.get("mixture")
     if refine:
@@ -672,6 +676,7 @@ def main():
         grids = e.nnp_autotune(reps=5) if not args.no_autotune else e.nnp_get_grids()
     wlog = e.run(args.warmup, log_interval=max(args.warmup, 1), graph=True)
     nbuild0 = wlog[-1]["nbuild"] if wlog else 0
+    nprune0 = e.prune_info()["nprune"]
 
     torch.cuda.synchronize()
     if dist:
@@ -689,6 +694,10 @@ def main():
     ms = max_over_ranks(t0.elapsed_time(t1), dist)
     info = e.list_info()
     nbuild_timed = (log[-1]["nbuild"] if log else info["nbuild"]) - nbuild0
+    pinfo = e.prune_info()
+    pruning = {"delta_A": round(pinfo["delta"], 3), "active": pinfo["active"],
+               "prunes_in_timed_steps": pinfo["nprune"] - nprune0,
+               "entries_per_atom": round(pinfo["entries"] / s.natom, 1) if pinfo["active"] else None}
     value = s.natom * args.steps * world / (ms / 1e3)
     launches = int(e.lib.nnpe_launches_per_step(e.h))
 
@@ -738,7 +747,8 @@ def main():
                 "traffic_unit": "bytes per launch (DRAM read+write, ncu)", "peak_source": src,
                 "kernel_ms": kms["network"], "alg_flops_per_launch": flops, "pairs_in_6A_per_atom": pairs6 / s.natom}
     else:
-        alg_bytes = s.natom * (4 * nlist + 48)
+        # the entries the pair kernel reads: the pruned copy's when pruning is on
+        alg_bytes = s.natom * (4 * (pruning["entries_per_atom"] or nlist) + 48)
         ach = alg_bytes / (kms["pair"] / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": "k_pair", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "traffic": profile_traffic([f"k_pair<0,0>:{args.workload}"]), "traffic_unit": "bytes per launch (DRAM read+write, ncu)",
@@ -812,6 +822,7 @@ def main():
                        "sample": f"unavailable: {ex}"}
         cfg = {"workload": args.workload, "description": wl["desc"], "natom": s.natom,
                "list_entries_per_atom": round(nlist, 1), "rebuilds_in_timed_steps": nbuild_timed,
+               "list_pruning": pruning,
                "l2": "inputs larger than L2 (neighbour list %.0f MB)" % (info["entries"] * 4 / 1e6),
                "ns_per_day": value / world / s.natom * 0.5 * 86400 * 1e-6, "kernel_ms": kms,
                "pair_math": "exact float sequence" if args.exact else "rsqrt+FMA (same cutoff test)"}

@@ -156,13 +156,24 @@ int nnpe_verlet_update_v(nnpe_ctx* ctx, double* ekin);
 int nnpe_list_build(nnpe_ctx* ctx);
 /* NEIGHLIST::isvalid (neighlist.cpp:178-187), AND over all atoms. */
 int nnpe_list_isvalid(nnpe_ctx* ctx, int* valid);
-/* update_ghost_pos<false> (environ.cpp:488-522). */
+/* update_ghost_pos<false> (environ.cpp:488-522); with pruning on (nnpe_set_prune), also remakes
+ * the pruned copy of the list when a rebuild or the displacement check asked for it. */
 int nnpe_ghost_update(nnpe_ctx* ctx);
 /* Sizes: natom, nghost, total list entries, nbuild. */
 int nnpe_list_info(nnpe_ctx* ctx, int* nghost, int64_t* nentries, int* nbuild, int* num_gx);
 /* Full list as records (atom id i, atom id j, image code, special class); image code
  * (sx+1)*9+(sy+1)*3+(sz+1) of the ghost shift, 13 for a real atom. cap = record capacity. */
 int nnpe_list_get(nnpe_ctx* ctx, int64_t cap, int* rec, int64_t* n);
+/* Dynamic pruning of the list (no counterpart in the reference, which evaluates every list entry;
+ * the pairs that interact are the same). With delta > 0 (and below the skin) the pair and network
+ * kernels read a copy of the list that keeps the entries within max(pair, network cutoff) + delta;
+ * it is remade after every rebuild and whenever an atom has moved delta/2 since it was made, so it
+ * holds every pair within the cutoffs. delta <= 0 or >= skin: off (the full list). Default 0.5 A.
+ * The g(r) tally and nnpe_list_get always use the full list. */
+int nnpe_set_prune(nnpe_ctx* ctx, double delta);
+/* delta, whether the copy is in use, how many copies were made since nnpe_setup, and the entries
+ * the current copy holds (any output may be null). */
+int nnpe_prune_info(nnpe_ctx* ctx, double* delta, int* active, int* nprune, int64_t* nentries);
 
 /* ---- forces (pair.cpp:289-419, bond/angle/dihedral compute, run.cpp:302-342) ------------
  * Clears the forces and evaluates pair + bonded (+ network when loaded) at the current

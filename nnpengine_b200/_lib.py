@@ -59,6 +59,8 @@ _SIGS = {
     "nnpe_list_isvalid": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "nnpe_ghost_update": (C.c_int, [_vp]),
     "nnpe_list_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "nnpe_set_prune": (C.c_int, [_vp, C.c_double]),
+    "nnpe_prune_info": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
     "nnpe_list_get": (C.c_int, [_vp, C.c_int64, _i32p, C.POINTER(C.c_int64)]),
     "nnpe_compute_forces": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nnpe_get_forces": (C.c_int, [_vp, C.c_int, _f32p]),

@@ -106,6 +106,7 @@ static void free_state(nnpe_ctx* c) {
   dfree(&c->d_perm); dfree(&c->d_gcnt); dfree(&c->d_goff); dfree(&c->d_gtmp_owner); dfree(&c->d_gtmp_shift);
   dfree(&c->d_gtmp_cell); dfree(&c->d_gtmp_slot); dfree(&c->d_sxd); dfree(&c->d_svd); dfree(&c->d_sacc);
   dfree(&c->d_sinfo); dfree(&c->d_satom); dfree(&c->d_sqm); dfree(&c->d_list); dfree(&c->d_ncount);
+  dfree(&c->d_plist); dfree(&c->d_pcount); dfree(&c->d_xprune);
   dfree(&c->d_eatom); dfree(&c->d_watom); dfree(&c->d_kin); dfree(&c->d_log);
   dfree(&c->d_xstage); dfree(&c->d_fstage);
   c->force_step_init = false;
@@ -366,10 +367,12 @@ int alloc_state(nnpe_ctx* c) {
   TRY(dalloc(c, &c->d_sxd, N)); TRY(dalloc(c, &c->d_svd, N)); TRY(dalloc(c, &c->d_sacc, N));
   TRY(dalloc(c, &c->d_sinfo, N)); TRY(dalloc(c, &c->d_satom, N)); TRY(dalloc(c, &c->d_sqm, N));
   TRY(dalloc(c, &c->d_list, (size_t)N * c->cap)); TRY(dalloc(c, &c->d_ncount, N));
+  TRY(dalloc(c, &c->d_plist, (size_t)N * c->cap)); TRY(dalloc(c, &c->d_pcount, N)); TRY(dalloc(c, &c->d_xprune, N));
   TRY(dalloc(c, &c->d_eatom, N)); TRY(dalloc(c, &c->d_watom, N)); TRY(dalloc(c, &c->d_kin, N));
   NNPE_CUDA(c, cudaMemset(c->d_eatom, 0, sizeof(double) * N));
   NNPE_CUDA(c, cudaMemset(c->d_watom, 0, sizeof(double) * N));
   NNPE_CUDA(c, cudaMemset(c->d_ncount, 0, sizeof(int) * N));
+  NNPE_CUDA(c, cudaMemset(c->d_pcount, 0, sizeof(int) * N));
   // info of real atoms in the current (atom-id or sorted) order
   std::vector<int> aid;
   TRY(get_atom_ids(c, aid));
@@ -643,6 +646,42 @@ int nnpe_list_info(nnpe_ctx* c, int* nghost, int64_t* nentries, int* nbuild, int
     int64_t s = 0;
     for (int v : cnt) s += v;
     *nentries = s;
+  }
+  return NNPE_OK;
+}
+
+int nnpe_set_prune(nnpe_ctx* c, double delta) {
+  if (!c || !(delta == delta) || delta > 1e3) return nnpe_fail(c, NNPE_EARG, "nnpe_set_prune: bad delta");
+  c->prune_delta = delta > 0 ? (float)delta : 0.f;
+  free_graphs(c);   // captured steps hold the list pointers of the old setting
+  if (c->d_ctrl) {  // the next evaluation makes a fresh copy
+    int one = 1;
+    NNPE_CUDA(c, cudaMemcpyAsync(c->d_ctrl + CTRL_PRUNE, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return NNPE_OK;
+}
+
+int nnpe_prune_info(nnpe_ctx* c, double* delta, int* active, int* nprune, int64_t* nentries) {
+  if (!c) return NNPE_EARG;
+  if (delta) *delta = c->prune_delta;
+  if (active) *active = prune_active(c) ? 1 : 0;
+  if (nentries) {
+    *nentries = 0;
+    if (c->d_pcount && prune_active(c)) {
+      std::vector<int> cnt(c->natom);
+      NNPE_CUDA(c, cudaMemcpyAsync(cnt.data(), c->d_pcount, sizeof(int) * c->natom, cudaMemcpyDeviceToHost, c->stream));
+      NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+      for (int v : cnt) *nentries += v;
+    }
+  }
+  if (nprune) {
+    *nprune = 0;
+    if (c->d_ctrl) {
+      NNPE_CUDA(c, cudaMemcpyAsync(c->h_ctrl, c->d_ctrl, sizeof(int) * CTRL_WORDS, cudaMemcpyDeviceToHost, c->stream));
+      NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+      *nprune = c->h_ctrl[CTRL_NPRUNE];
+    }
   }
   return NNPE_OK;
 }

@@ -418,7 +418,7 @@ bool nnp_list6(nnpe_ctx* c, uint32_t** list6, int** n6, int* cap6, float* cut6);
 int pair_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   const int N = c->natom;
   PairParams p;
-  p.pos = c->d_pos; p.list = c->d_list; p.ncount = c->d_ncount; p.info = c->d_info; p.table = c->d_table;
+  p.pos = c->d_pos; p.list = force_list(c); p.ncount = force_count(c); p.info = c->d_info; p.table = c->d_table;
   p.gowner = c->d_gowner; p.gshift = c->d_gshift; p.g = c->grid;
   p.pairtype = c->d_pairtype; p.frc = c->d_frc; p.eatom = c->d_eatom; p.watom = c->d_watom;
   p.N = N; p.cap = c->cap; p.ntype = c->ntype; p.nbin = c->nbin;

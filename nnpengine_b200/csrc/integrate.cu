@@ -22,10 +22,11 @@ constexpr double kKB300 = 0.5961612775922496;
 
 // updateX (verlet.cpp:305-319): x += (v + a*hdt)*dt; the acceleration array doubles as f_prev.
 // Also refreshes the FP32 coordinates and flags the list for rebuild when an atom moved more than
-// skin/2 since the last build (NEIGHLIST::isvalid, neighlist.cpp:178-187).
+// skin/2 since the last build (NEIGHLIST::isvalid, neighlist.cpp:178-187); with xprune, flags the
+// pruned copy of the list when an atom moved more than prune_delta/2 since the last prune.
 __global__ void k_update_x(double4* __restrict__ xd, const double4* __restrict__ vd, const float4* __restrict__ acc,
-                           float4* __restrict__ pos, const float4* __restrict__ xbuild, int N, float dt, double dt64,
-                           bool fp64, bool check, float dx2, int* ctrl) {
+                           float4* __restrict__ pos, const float4* __restrict__ xbuild, const float4* __restrict__ xprune,
+                           int N, float dt, double dt64, bool fp64, bool check, float dx2, float pdx2, int* ctrl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double4 x = xd[i];
@@ -52,6 +53,11 @@ __global__ void k_update_x(double4* __restrict__ xd, const double4* __restrict__
     const float4 b = xbuild[i];
     const float ex = xf - b.x, ey = yf - b.y, ez = zf - b.z;
     if (ex * ex + ey * ey + ez * ez > dx2) ctrl[CTRL_REBUILD] = 1;
+    if (xprune) {
+      const float4 p = xprune[i];
+      const float px = xf - p.x, py = yf - p.y, pz = zf - p.z;
+      if (px * px + py * py + pz * pz > pdx2) ctrl[CTRL_PRUNE] = 1;
+    }
   }
 }
 
@@ -164,8 +170,9 @@ __global__ void k_init_pos(const double4* __restrict__ xd, const float2* __restr
 
 int verlet_x_enqueue(nnpe_ctx* c, double dt, bool check) {
   const float h = c->skin / 2;
-  k_update_x<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_xd, c->d_vd, c->d_acc, c->d_pos, c->d_xbuild, c->natom,
-                                                            (float)dt, dt, c->fp64_state, check, h * h, c->d_ctrl);
+  k_update_x<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_xd, c->d_vd, c->d_acc, c->d_pos, c->d_xbuild,
+                                                            prune_active(c) ? c->d_xprune : nullptr, c->natom, (float)dt,
+                                                            dt, c->fp64_state, check, h * h, prune_dx2(c), c->d_ctrl);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

@@ -30,7 +30,10 @@ enum {
   CTRL_NBUILD = 3,
   CTRL_STEP = 4,
   CTRL_NLOG = 5,
-  CTRL_WORDS = 8
+  CTRL_PRUNE = 6,        // the pruned list is stale: set by a rebuild or a displacement past delta/2
+  CTRL_PRUNE_DONE = 7,   // blocks of k_prune that finished (the last one clears CTRL_PRUNE)
+  CTRL_NPRUNE = 8,       // prunes so far
+  CTRL_WORDS = 12
 };
 
 struct GridParams {
@@ -124,6 +127,13 @@ struct nnpe_ctx {
   // list
   uint32_t* d_list = nullptr;
   int* d_ncount = nullptr;
+  // dynamically pruned copy of the list (the pairs within the force cutoff + prune_delta at the
+  // last prune) and the positions at that prune; the pair and network kernels read it while no
+  // atom has moved prune_delta/2 since (prune_delta <= 0 or >= skin: off, they read the full list)
+  uint32_t* d_plist = nullptr;
+  int* d_pcount = nullptr;
+  float4* d_xprune = nullptr;
+  float prune_delta = 0.5f;
   // energies
   double *d_eatom = nullptr, *d_watom = nullptr, *d_kin = nullptr;   // per atom
   double *d_emol = nullptr, *d_wmol = nullptr;                         // per molecule
@@ -225,6 +235,12 @@ int gr_tally_enqueue(nnpe_ctx* c, int inner);
 int alloc_state(nnpe_ctx* c);
 int build_stencil_host(nnpe_ctx* c, float cutoff, int max_nbin, Stencil* out);
 int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6 = true);
+// Dynamic pruning of the list (rebuild.cu). The pair and network kernels read force_list() /
+// force_count(): the pruned copy while pruning is on, else the full list.
+bool prune_active(const nnpe_ctx* c);
+const uint32_t* force_list(const nnpe_ctx* c);
+const int* force_count(const nnpe_ctx* c);
+float prune_dx2(const nnpe_ctx* c);   // (prune_delta/2)^2, the displacement that makes the copy stale
 // The host-positions force step (nnpe_force_step) with its staging buffers given by the caller:
 // xstage and fstage hold at least 3 * natom floats each on the context's device. graph: launch the
 // device part as the context's cached CUDA graph (else kernel by kernel).

@@ -918,7 +918,7 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   cudaStream_t st = c->stream;
   const float cs = m->rc * m->rc;
   if (filter6)   // else the pair kernel of this step has filled the list (forces.cu)
-    k_filter6<<<nblocks((long)N * 32, 128), 128, 0, st>>>(c->d_pos, c->d_list, c->d_ncount, c->cap, m->d_list6, m->d_n6,
+    k_filter6<<<nblocks((long)N * 32, 128), 128, 0, st>>>(c->d_pos, force_list(c), force_count(c), c->cap, m->d_list6, m->d_n6,
                                                         m->cap6, cs, N, c->d_ctrl);
   if (int rc = nnp_species_enqueue(c)) return rc;
   NnpArgs a = make_args(c);

@@ -324,16 +324,77 @@ __global__ void k_finish_rebuild(int* ctrl) {
   if (ctrl[CTRL_REBUILD]) {
     ctrl[CTRL_REBUILD] = 0;
     ctrl[CTRL_NBUILD] += 1;
+    ctrl[CTRL_PRUNE] = 1;   // a new list: the pruned copy is made from it before the forces
   }
 }
 
-// isvalid: any atom displaced more than skin/2 since the last build (neighlist.cpp:178-187).
-__global__ void k_check_valid(const float4* __restrict__ pos, const float4* __restrict__ xbuild, int N, float dx2,
-                              int* ctrl) {
+// isvalid: any atom displaced more than skin/2 since the last build (neighlist.cpp:178-187); with
+// xprune, also more than prune_delta/2 since the last prune (the pruned copy is then stale).
+__global__ void k_check_valid(const float4* __restrict__ pos, const float4* __restrict__ xbuild,
+                              const float4* __restrict__ xprune, int N, float dx2, float pdx2, int* ctrl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const float4 a = pos[i], b = xbuild[i];
   if (rsq3(fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)) > dx2) ctrl[CTRL_REBUILD] = 1;
+  if (xprune) {
+    const float4 p = xprune[i];
+    if (rsq3(fsub(a.x, p.x), fsub(a.y, p.y), fsub(a.z, p.z)) > pdx2) ctrl[CTRL_PRUNE] = 1;
+  }
+}
+
+// Dynamic pruning. The Verlet list holds every pair within cutoff + skin of the last build; most
+// of its outer shell is beyond the force cutoff at any one step, yet the pair kernel evaluates
+// every entry. When CTRL_PRUNE is set (a rebuild, or an atom displaced more than delta/2 since the
+// last prune), this kernel copies each atom's row keeping the entries within cutoff + delta at the
+// current positions, in list order, and records those positions. Until an atom moves delta/2, a
+// pair beyond cutoff + delta then cannot come within the cutoff (each of its atoms moved less than
+// delta/2), so the copy holds every pair the forces need. One warp per atom (grid-stride); without
+// the flag every block returns at once. The last block to finish clears the flag, after every block
+// has read it.
+__global__ void __launch_bounds__(256) k_prune(const float4* __restrict__ pos, const uint32_t* __restrict__ list,
+                                               const int* __restrict__ ncount, int cap, uint32_t* __restrict__ plist,
+                                               int* __restrict__ pcount, float4* __restrict__ xprune, int N, float cutsq,
+                                               int* ctrl) {
+  if (*reinterpret_cast<volatile int*>(ctrl + CTRL_PRUNE) == 0) return;   // block-uniform
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += nw) {   // warp-uniform
+    const float4 xi = pos[i];
+    const uint32_t* row = list + (size_t)i * cap;
+    uint32_t* out = plist + (size_t)i * cap;
+    const int n = ncount[i];
+    int cnt = 0;
+    // software pipeline over 32-entry chunks: entries two chunks ahead and neighbour positions one
+    // chunk ahead are in flight while a chunk is tested
+    uint32_t e_nx = lane < n ? __ldg(row + lane) : 0u;
+    uint32_t e_nx2 = lane + 32 < n ? __ldg(row + lane + 32) : 0u;
+    float4 x_nx = lane < n ? __ldg(pos + (e_nx & NNPE_J_MASK)) : xi;
+    for (int base = 0; base < n; base += 32) {
+      const int k = base + lane;
+      const uint32_t e = e_nx;
+      const float4 xj = x_nx;
+      e_nx = e_nx2;
+      x_nx = k + 32 < n ? __ldg(pos + (e_nx & NNPE_J_MASK)) : xi;
+      e_nx2 = k + 64 < n ? __ldg(row + k + 64) : 0u;
+      const bool keep = k < n && rsq3(fsub(xi.x, xj.x), fsub(xi.y, xj.y), fsub(xi.z, xj.z)) < cutsq;
+      const unsigned b = __ballot_sync(0xffffffffu, keep);
+      if (keep) out[cnt + __popc(b & ((1u << lane) - 1))] = e;
+      cnt += __popc(b);
+    }
+    if (lane == 0) {
+      pcount[i] = cnt;
+      xprune[i] = xi;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(reinterpret_cast<unsigned*>(ctrl + CTRL_PRUNE_DONE), 1u) == gridDim.x - 1) {
+      ctrl[CTRL_PRUNE] = 0;
+      ctrl[CTRL_PRUNE_DONE] = 0;
+      ctrl[CTRL_NPRUNE] += 1;
+    }
+  }
 }
 
 }  // namespace
@@ -371,17 +432,41 @@ int rebuild_enqueue(nnpe_ctx* c, bool cond) {
   return 0;
 }
 
+bool prune_active(const nnpe_ctx* c) { return c->d_plist && c->prune_delta > 0.f && c->prune_delta < c->skin; }
+const uint32_t* force_list(const nnpe_ctx* c) { return prune_active(c) ? c->d_plist : c->d_list; }
+const int* force_count(const nnpe_ctx* c) { return prune_active(c) ? c->d_pcount : c->d_ncount; }
+float prune_dx2(const nnpe_ctx* c) {
+  const float h = 0.5f * c->prune_delta;
+  return h * h;
+}
+
+float nnp_cutoff(nnpe_ctx* c);   // nnp.cu
+
+// With pruning on, the pruned copy of the list, remade on the device when CTRL_PRUNE is set; it
+// follows every ghost update (the images must hold this step's positions), so that every force
+// evaluation reads a current copy.
+static void prune_enqueue(nnpe_ctx* c) {
+  if (!prune_active(c)) return;
+  const float rc = std::max(c->pair_cutoff, c->nnp ? nnp_cutoff(c) : 0.f) + c->prune_delta;
+  const int blocks = std::max(1, std::min(nblocks((long)c->natom * 32, 256), 8 * nnpe_sm_count(c->device)));
+  k_prune<<<blocks, 256, 0, c->stream>>>(c->d_pos, c->d_list, c->d_ncount, c->cap, c->d_plist, c->d_pcount, c->d_xprune,
+                                         c->natom, rc * rc, c->d_ctrl);
+}
+
+// The ghost images of this step's positions, the end of a rebuild and the pruned copy of the list.
 int ghost_update_enqueue(nnpe_ctx* c, bool) {
   k_ghost_update<<<nblocks(c->Gcap, 256), 256, 0, c->stream>>>(c->d_pos, c->d_gowner, c->d_gshift, c->natom, c->Gcap,
                                                                c->grid, c->d_ctrl);
   k_finish_rebuild<<<1, 1, 0, c->stream>>>(c->d_ctrl);
+  prune_enqueue(c);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }
 
 int check_valid_enqueue(nnpe_ctx* c) {
   const float h = c->skin / 2;
-  k_check_valid<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_pos, c->d_xbuild, c->natom, h * h, c->d_ctrl);
+  k_check_valid<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_pos, c->d_xbuild, prune_active(c) ? c->d_xprune : nullptr,
+                                                               c->natom, h * h, prune_dx2(c), c->d_ctrl);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }
@@ -430,6 +515,7 @@ extern "C" int nnpe_ghost_update(nnpe_ctx* c) {
   if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_ghost_update");
   k_ghost_update<<<nblocks(c->Gcap, 256), 256, 0, c->stream>>>(c->d_pos, c->d_gowner, c->d_gshift, c->natom, c->Gcap,
                                                                c->grid, c->d_ctrl);
+  prune_enqueue(c);
   NNPE_CHECK_LAUNCH(c);
   return NNPE_OK;
 }

@@ -98,13 +98,14 @@ void copy_opt(std::vector<float>& dst, const float* src, size_t n) {
 const float* ptr_or_null(const std::vector<float>& v) { return v.empty() ? nullptr : v.data(); }
 
 // Device bytes of a replica before it exists (the admission test; the measured figure replaces it
-// once the replica is set up): the neighbour list (natom * neigh_cap int32) dominates; per-atom
+// once the replica is set up): the neighbour list and its pruned copy (2 * natom * neigh_cap int32)
+// dominate; per-atom
 // state and sort scratch (~400 B); periodic images within skin + cutoff of the faces (~64 B each:
 // positions, info, cell, owner, shift and sort scratch), which outnumber the atoms in boxes not
 // much larger than the cutoff; with the network term its pair list and descriptor buffers; and a
 // fixed part (tables, weight images, graphs).
 int64_t footprint_estimate(const nnpe_serve_config& c, int natom, double bl) {
-  int64_t per_atom = (int64_t)c.neigh_cap * 4 + 400;
+  int64_t per_atom = (int64_t)c.neigh_cap * 4 * 2 + 420;   // the list and its pruned copy
   if (c.nnp_kind >= 0) per_atom += 256 * 4 + 2 * 256 * 4 + 64;
   const double comm = c.skin + c.pair_cutoff, g = (bl + 2 * comm) / bl;
   const double images = std::min((double)natom * (g * g * g - 1) * 1.2 + 4096, 26.0 * natom + 4096);

@@ -229,6 +229,15 @@ class Engine:
         self._ok(self.lib.nnpe_list_info(self.h, C.byref(ng), C.byref(ne), C.byref(nb), C.byref(gx)))
         return dict(nghost=ng.value, entries=ne.value, nbuild=nb.value, num_gx=gx.value)
 
+    def set_prune(self, delta: float) -> None:
+        """Dynamic list pruning margin in A (<= 0 or >= skin: off, the kernels read the full list)."""
+        self._ok(self.lib.nnpe_set_prune(self.h, float(delta)))
+
+    def prune_info(self) -> Dict[str, float]:
+        d, a, n, ne = C.c_double(0), C.c_int(0), C.c_int(0), C.c_int64(0)
+        self._ok(self.lib.nnpe_prune_info(self.h, C.byref(d), C.byref(a), C.byref(n), C.byref(ne)))
+        return dict(delta=d.value, active=bool(a.value), nprune=n.value, entries=ne.value)
+
     def list_records(self) -> np.ndarray:
         n = self.list_info()["entries"]
         rec = np.zeros(4 * max(n, 1), np.int32)
