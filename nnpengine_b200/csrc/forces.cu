@@ -17,8 +17,15 @@ struct PairParams {
   const int* gowner;
   const int* gshift;
   GridParams g;
-  const uint32_t* list;
+  const uint32_t* list;     // the full list
   const int* ncount;
+  // the pruned copy (nullptr: pruning off). The pass reads it, or, when CTRL_PRUNE is set at its
+  // start, reads the full list and remakes it (entries with rsq < prunesq, in list order) with the
+  // positions of this pass.
+  uint32_t* plist;
+  int* pcount;
+  float4* xprune;
+  float prunesq;
   const int2* info;
   const float2* table;
   const int* pairtype;
@@ -79,19 +86,19 @@ __device__ __forceinline__ void pair_energy64(const PairParams& p, const float2*
 // contraction), bit-identical per pair. EXACT=false keeps the same cutoff test (so the same pairs
 // interact) but uses rsqrt and fused multiply-adds: ~1 ulp per pair, forces within 1e-6 relative.
 template <bool EV, bool EXACT>
-__global__ void __launch_bounds__(128) k_pair(PairParams p) {
-  const int lane = threadIdx.x & 31;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (i >= p.N) return;
+__device__ __forceinline__ void pair_row(const PairParams& p, int i, int lane, bool reprune) {
   const float4 xi = p.pos[i];
   const int ti = p.info[i].y & 0xFF;
   const int* ptrow = p.pairtype + ti * p.ntype;
-  const uint32_t* row = p.list + (size_t)i * p.cap;
-  const int n = p.ncount[i];
+  const bool full = reprune || !p.plist;
+  const uint32_t* row = (full ? p.list : p.plist) + (size_t)i * p.cap;
+  const int n = full ? p.ncount[i] : p.pcount[i];
   float fx = 0.f, fy = 0.f, fz = 0.f;
   double e = 0.0, w = 0.0;
   uint32_t* out6 = p.list6 ? p.list6 + (size_t)i * p.cap6 : nullptr;
   int cnt6 = 0;
+  uint32_t* outp = reprune ? p.plist + (size_t)i * p.cap : nullptr;
+  int cntp = 0;
   // software pipeline over 32-entry chunks: the list entries two chunks ahead and the neighbour
   // positions one chunk ahead are in flight while a chunk is evaluated
   uint32_t e_nx = lane < n ? __ldg(row + lane) : 0u;
@@ -116,6 +123,12 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
         if (idx < p.cap6) out6[idx] = ent;
       }
       cnt6 += __popc(b6);
+    }
+    if (outp) {   // warp-uniform
+      const bool kp = in && rsq < p.prunesq;
+      const unsigned bp = __ballot_sync(0xffffffffu, kp);
+      if (kp) outp[cntp + __popc(bp & ((1u << lane) - 1))] = ent;
+      cntp += __popc(bp);
     }
     if (!in) continue;
     if (rsq < p.cutsq) {
@@ -168,6 +181,10 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
     p.n6[i] = min(cnt6, p.cap6);
     if (cnt6 > p.cap6) atomicOr(p.ctrl + CTRL_ERR, NNPE_DEV_LIST_OVERFLOW);
   }
+  if (outp && lane == 0) {
+    p.pcount[i] = cntp;
+    p.xprune[i] = xi;
+  }
   if (lane == 0) {
     if (p.accumulate) {
       float4 f = p.frc[i];
@@ -180,6 +197,18 @@ __global__ void __launch_bounds__(128) k_pair(PairParams p) {
       p.watom[i] = p.accumulate ? p.watom[i] + w : w;
     }
   }
+}
+
+// With pruning on, the pass reads the pruned copy of the list; on the steps that asked for a new
+// copy (a rebuild, or an atom displaced prune_delta/2 since the last copy) it reads the full list
+// instead and remakes the copy from the distances it computes anyway.
+template <bool EV, bool EXACT>
+__global__ void __launch_bounds__(128) k_pair(PairParams p) {
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const bool reprune = p.plist && *reinterpret_cast<volatile int*>(p.ctrl + CTRL_PRUNE) != 0;   // grid-uniform
+  if (i < p.N) pair_row<EV, EXACT>(p, i, lane, reprune);
+  if (reprune) prune_pass_done(p.ctrl);
 }
 
 __global__ void k_zero_forces(float4* frc, double* eatom, double* watom, int N) {
@@ -418,7 +447,10 @@ bool nnp_list6(nnpe_ctx* c, uint32_t** list6, int** n6, int* cap6, float* cut6);
 int pair_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   const int N = c->natom;
   PairParams p;
-  p.pos = c->d_pos; p.list = force_list(c); p.ncount = force_count(c); p.info = c->d_info; p.table = c->d_table;
+  p.pos = c->d_pos; p.list = c->d_list; p.ncount = c->d_ncount; p.info = c->d_info; p.table = c->d_table;
+  const bool pr = prune_in_pair(c);
+  p.plist = pr ? c->d_plist : nullptr; p.pcount = pr ? c->d_pcount : nullptr; p.xprune = pr ? c->d_xprune : nullptr;
+  p.prunesq = pr ? prune_cutsq(c) : 0.f;
   p.gowner = c->d_gowner; p.gshift = c->d_gshift; p.g = c->grid;
   p.pairtype = c->d_pairtype; p.frc = c->d_frc; p.eatom = c->d_eatom; p.watom = c->d_watom;
   p.N = N; p.cap = c->cap; p.ntype = c->ntype; p.nbin = c->nbin;

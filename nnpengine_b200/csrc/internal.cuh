@@ -240,7 +240,24 @@ int nnp_forces_enqueue(nnpe_ctx* c, bool ev, bool filter6 = true);
 bool prune_active(const nnpe_ctx* c);
 const uint32_t* force_list(const nnpe_ctx* c);
 const int* force_count(const nnpe_ctx* c);
-float prune_dx2(const nnpe_ctx* c);   // (prune_delta/2)^2, the displacement that makes the copy stale
+float prune_dx2(const nnpe_ctx* c);     // (prune_delta/2)^2, the displacement that makes the copy stale
+float prune_cutsq(const nnpe_ctx* c);   // (max(pair, network cutoff) + prune_delta)^2, what the copy keeps
+// The pair kernel remakes the copy itself in the pass that reads the full list (when it runs in
+// the force evaluation); else a separate pass after the ghost update does.
+bool prune_in_pair(const nnpe_ctx* c);
+// End of a pass that remade the pruned copy (CTRL_PRUNE was set at its start, block-uniformly):
+// the last block to finish clears the request, after every block has read it.
+static __device__ __forceinline__ void prune_pass_done(int* ctrl) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(reinterpret_cast<unsigned*>(ctrl + CTRL_PRUNE_DONE), 1u) == gridDim.x - 1) {
+      ctrl[CTRL_PRUNE] = 0;
+      ctrl[CTRL_PRUNE_DONE] = 0;
+      ctrl[CTRL_NPRUNE] += 1;
+    }
+  }
+}
 // The host-positions force step (nnpe_force_step) with its staging buffers given by the caller:
 // xstage and fstage hold at least 3 * natom floats each on the context's device. graph: launch the
 // device part as the context's cached CUDA graph (else kernel by kernel).

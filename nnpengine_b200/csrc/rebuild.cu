@@ -386,15 +386,7 @@ __global__ void __launch_bounds__(256) k_prune(const float4* __restrict__ pos, c
       xprune[i] = xi;
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(reinterpret_cast<unsigned*>(ctrl + CTRL_PRUNE_DONE), 1u) == gridDim.x - 1) {
-      ctrl[CTRL_PRUNE] = 0;
-      ctrl[CTRL_PRUNE_DONE] = 0;
-      ctrl[CTRL_NPRUNE] += 1;
-    }
-  }
+  prune_pass_done(ctrl);
 }
 
 }  // namespace
@@ -439,18 +431,22 @@ float prune_dx2(const nnpe_ctx* c) {
   const float h = 0.5f * c->prune_delta;
   return h * h;
 }
-
 float nnp_cutoff(nnpe_ctx* c);   // nnp.cu
+float prune_cutsq(const nnpe_ctx* c) {
+  const float rc = std::max(c->pair_cutoff, c->nnp ? nnp_cutoff(const_cast<nnpe_ctx*>(c)) : 0.f) + c->prune_delta;
+  return rc * rc;
+}
+bool prune_in_pair(const nnpe_ctx* c) { return prune_active(c) && c->pair_on && c->d_table; }
 
-// With pruning on, the pruned copy of the list, remade on the device when CTRL_PRUNE is set; it
+// With pruning on, the pruned copy of the list, remade on the device when CTRL_PRUNE is set. It
 // follows every ghost update (the images must hold this step's positions), so that every force
-// evaluation reads a current copy.
+// evaluation reads a current copy; when the pair kernel runs in the force evaluation, that kernel
+// remakes the copy in its own pass over the full list instead (prune_in_pair).
 static void prune_enqueue(nnpe_ctx* c) {
-  if (!prune_active(c)) return;
-  const float rc = std::max(c->pair_cutoff, c->nnp ? nnp_cutoff(c) : 0.f) + c->prune_delta;
+  if (!prune_active(c) || prune_in_pair(c)) return;
   const int blocks = std::max(1, std::min(nblocks((long)c->natom * 32, 256), 8 * nnpe_sm_count(c->device)));
   k_prune<<<blocks, 256, 0, c->stream>>>(c->d_pos, c->d_list, c->d_ncount, c->cap, c->d_plist, c->d_pcount, c->d_xprune,
-                                         c->natom, rc * rc, c->d_ctrl);
+                                         c->natom, prune_cutsq(c), c->d_ctrl);
 }
 
 // The ghost images of this step's positions, the end of a rebuild and the pruned copy of the list.
