@@ -33,6 +33,8 @@ enum {
   CTRL_PRUNE = 6,        // the pruned list is stale: set by a rebuild or a displacement past delta/2
   CTRL_PRUNE_DONE = 7,   // blocks of k_prune that finished (the last one clears CTRL_PRUNE)
   CTRL_NPRUNE = 8,       // prunes so far
+  CTRL_RESORT = 9,       // the sorted order changed (a rebuild, or a new network): species lists are stale
+  CTRL_RESORT_DONE = 10, // blocks of k_species that finished (the last one clears CTRL_RESORT)
   CTRL_WORDS = 12
 };
 

@@ -194,6 +194,12 @@ int nnpe_nnp_set(nnpe_ctx* c, int kind, double cutoff, int nbin, double scale, i
   for (int t = 0; t < c->ntype; ++t) m->soff[t + 1] = m->soff[t] + cnt[t];
   if ((rc = nalloc(c, &m->d_soff_dev, NNPE_MAX_TYPES + 1))) return rc;
   NNPE_CUDA(c, cudaMemcpy(m->d_soff_dev, m->soff.data(), sizeof(int) * m->soff.size(), cudaMemcpyHostToDevice));
+  // species lists: counters start at zero, and the next evaluation builds the lists (k_species)
+  NNPE_CUDA(c, cudaMemset(m->d_scount, 0, sizeof(int) * NNPE_MAX_TYPES));
+  {
+    const int one = 1;
+    NNPE_CUDA(c, cudaMemcpy(c->d_ctrl + CTRL_RESORT, &one, sizeof(int), cudaMemcpyHostToDevice));
+  }
   if (kind == 1) {
     const size_t eb = (size_t)32 + 32 + 32 * (size_t)e2 + e2;
     const int smem_desc = (int)(sizeof(float) * (eb * c->ntype + kEmbWarpsHost * kDescScratchHost));
@@ -255,9 +261,12 @@ __global__ void __launch_bounds__(128) k_filter6(const float4* __restrict__ pos,
 
 // Species membership lists (sorted atom indices grouped by type) for the per-species fitting net.
 // (The order within a species is arbitrary: every fitting row depends on its own atom only.)
-// One counter update per warp and species.
+// One counter update per warp and species. The lists change only with the sorted order, so the
+// kernel works only when CTRL_RESORT is set (a rebuild or a new network) and returns at once
+// otherwise; the last block to finish clears the flag and the counters (zero for the next time).
 __global__ void k_species(const int2* __restrict__ info, int* __restrict__ sidx, int* __restrict__ scount,
-                          const int* __restrict__ soff, int N, int ntype) {
+                          const int* __restrict__ soff, int N, int ntype, int* ctrl) {
+  if (*reinterpret_cast<volatile int*>(ctrl + CTRL_RESORT) == 0) return;   // grid-uniform
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int t = i < N ? (info[i].y & 0xFF) : -1;
@@ -269,6 +278,15 @@ __global__ void k_species(const int2* __restrict__ info, int* __restrict__ sidx,
     if (lane == leader) base = atomicAdd(&scount[sp], __popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (t == sp) sidx[soff[sp] + base + __popc(m & ((1u << lane) - 1))] = i;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(reinterpret_cast<unsigned*>(ctrl + CTRL_RESORT_DONE), 1u) == gridDim.x - 1) {
+      for (int sp = 0; sp < ntype; ++sp) scount[sp] = 0;
+      ctrl[CTRL_RESORT] = 0;
+      ctrl[CTRL_RESORT_DONE] = 0;
+    }
   }
 }
 
@@ -905,9 +923,8 @@ static int fit_f32_enqueue(nnpe_ctx* c) {
 
 int nnp_species_enqueue(nnpe_ctx* c) {
   NnpModel* m = c->nnp;
-  NNPE_CUDA(c, cudaMemsetAsync(m->d_scount, 0, sizeof(int) * NNPE_MAX_TYPES, c->stream));
   k_species<<<nblocks(c->natom, 256), 256, 0, c->stream>>>(c->d_info, m->d_sidx, m->d_scount, m->d_soff_dev, c->natom,
-                                                          c->ntype);
+                                                          c->ntype, c->d_ctrl);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }

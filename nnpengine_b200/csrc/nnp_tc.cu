@@ -744,18 +744,23 @@ __global__ void __launch_bounds__(256, 2) k_tc_force2(ForceArgs a) {
   if (w == 0) tc::tmem_dealloc(tmem, 256);
 }
 
-// frc[i] += network force of atom i, watom[i] += its virial (EV), from the [N][4] fixed-point sums.
+// frc[i] += network force of atom i, watom[i] += its virial (EV), from the [N][4] fixed-point sums,
+// which are left zeroed for the next force kernel (the buffer starts zeroed at set-up).
 template <bool EV>
-__global__ void k_facc_apply4(const unsigned long long* __restrict__ facc, float4* __restrict__ frc, double* watom, int N) {
+__global__ void k_facc_apply4(unsigned long long* __restrict__ facc, float4* __restrict__ frc, double* watom, int N) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const double s = 1.0 / kFix;
+  ulonglong2* q = reinterpret_cast<ulonglong2*>(facc + 4 * (size_t)i);
+  const ulonglong2 a = q[0], b = q[1];
+  q[0] = make_ulonglong2(0ull, 0ull);
+  q[1] = make_ulonglong2(0ull, 0ull);
   float4 f = frc[i];
-  f.x += (float)((double)(long long)facc[4 * i] * s);
-  f.y += (float)((double)(long long)facc[4 * i + 1] * s);
-  f.z += (float)((double)(long long)facc[4 * i + 2] * s);
+  f.x += (float)((double)(long long)a.x * s);
+  f.y += (float)((double)(long long)a.y * s);
+  f.z += (float)((double)(long long)b.x * s);
   frc[i] = f;
-  if (EV) watom[i] += (double)(long long)facc[4 * i + 3] * s;
+  if (EV) watom[i] += (double)(long long)b.y * s;
 }
 
 // -------------------------------------------------------------------------------------------
@@ -1018,6 +1023,7 @@ int nnp_tc_setup(nnpe_ctx* c) {
   };
   if (int rc = up((void**)&t->d_wdesc64, wdesc64.data(), wdesc64.size() * 2)) return rc;
   NNPE_CUDA(c, dev_malloc(c, (void**)&t->d_facc, sizeof(unsigned long long) * 4 * std::max(c->natom, 1)));
+  NNPE_CUDA(c, cudaMemset(t->d_facc, 0, sizeof(unsigned long long) * 4 * std::max(c->natom, 1)));   // the apply re-zeroes it
   if (int rc = up((void**)&t->d_fit, fit.data(), fit.size() * 2)) return rc;
   if (int rc = up((void**)&t->d_emb_small, emb_small.data(), emb_small.size() * 4)) return rc;
   if (int rc = up((void**)&t->d_fit_small, fit_small.data(), fit_small.size() * 4)) return rc;
@@ -1052,7 +1058,6 @@ int nnp_tc_forces_enqueue(nnpe_ctx* c, bool ev) {
   f.fit = t->d_fit; f.fit_stride = t->fit_stride; f.small = t->d_fit_small; f.dG = m->d_dG; f.enet = m->d_enet;
   f.ctrl = c->d_ctrl;
   k_tc_fit<<<t->ntiles, 256, smem_fit, c->stream>>>(f);
-  NNPE_CUDA(c, cudaMemsetAsync(t->d_facc, 0, sizeof(unsigned long long) * 4 * c->natom, c->stream));
   ForceArgs fa;
   fa.pos = c->d_pos; fa.list6 = m->d_list6; fa.n6 = m->d_n6; fa.gowner = c->d_gowner; fa.wdesc = t->d_wdesc64;
   fa.emb_small = t->d_emb_small; fa.dG = m->d_dG; fa.facc = t->d_facc; fa.ctrl = c->d_ctrl;

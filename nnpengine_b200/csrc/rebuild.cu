@@ -325,6 +325,7 @@ __global__ void k_finish_rebuild(int* ctrl) {
     ctrl[CTRL_REBUILD] = 0;
     ctrl[CTRL_NBUILD] += 1;
     ctrl[CTRL_PRUNE] = 1;   // a new list: the pruned copy is made from it before the forces
+    ctrl[CTRL_RESORT] = 1;  // a new order: the network's species lists follow it
   }
 }
 
