@@ -823,6 +823,7 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   __shared__ uint64_t bar, bar_w[2];
   __shared__ uint32_t tmem_base;
   __shared__ float sEn[2][128];             // per-half partial energies
+  __shared__ __align__(16) float sSmall[kFitSmallStride];   // this species' c1, c2, a3, c3
   unsigned char* sAct = sm;                 // 128 x 256 (G), later 128 x 128 (g2)
   unsigned char* sH1 = sm + 128 * 256 * 2;  // 128 x 128 (h1, later g1)
   unsigned char* sW0 = sH1 + 128 * 128 * 2; // L1 image (K-major A1; MN-major it is A1^T for B1)
@@ -833,7 +834,8 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   const bool valid = row0 + p < M;
   const int atom = valid ? f.sidx[f.soff[sp] + row0 + p] : 0;
   const unsigned char* img = f.fit + f.fit_stride * sp;
-  const float* sm_c1 = f.small + kFitSmallStride * sp;
+  for (int k = t; k < kFitSmallStride; k += 256) sSmall[k] = __ldg(f.small + kFitSmallStride * sp + k);
+  const float* sm_c1 = sSmall;   // read after the barrier below
   const float *sm_c2 = sm_c1 + 128, *sm_c3 = sm_c1 + 384, *sm_a3 = sm_c1 + 256;
   int issued0 = 0, issued1 = 0;             // bulk loads per buffer (thread 0)
   if (w == 0) tc::tmem_alloc(&tmem_base, 256);
@@ -866,30 +868,30 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   // L1: z1 = G A1 (+c1), h1 = tanh
   ok = fit_mma(tmem, aAct, 256, aW0, 128, &bar, 0, &bar_w[0], 0, t, f.ctrl);
   if (ok) {
-    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
-      float v[16];
-      tc::tmem_ld16(taddr + c0, v);
+    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 32) {   // two 16-column loads behind one wait
+      float v[32];
+      tc::tmem_ld16x2(taddr + c0, taddr + c0 + 16, v, v + 16);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) v[q] = tanh_fast(v[q] + sm_c1[c0 + q]);
-      *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0, 128)) = tc::pack8(v);
-      *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0 + 8, 128)) = tc::pack8(v + 8);
+      for (int q = 0; q < 32; ++q) v[q] = tanh_fast(v[q] + sm_c1[c0 + q]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) *reinterpret_cast<uint4*>(sH1 + tc::kmajor_off(p, c0 + 8 * k, 128)) = tc::pack8(v + 8 * k);
     }
   }
   // L2: z2 = h1 A2 (+c2), h2 = tanh, E = h2 A3 + c3, g2 = A3 (1-h2^2)
   if (ok) ok = fit_mma(tmem + 128, aH1, 128, aW1, 128, &bar, 1, &bar_w[1], 0, t, f.ctrl);
   if (ok) {
     float e = 0.f;
-    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 16) {
-      float v[16];
-      tc::tmem_ld16(taddr + 128 + c0, v);
+    for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 32) {
+      float v[32];
+      tc::tmem_ld16x2(taddr + 128 + c0, taddr + 128 + c0 + 16, v, v + 16);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
+      for (int q = 0; q < 32; ++q) {
         const float h2 = tanh_fast(v[q] + sm_c2[c0 + q]);
         e += h2 * sm_a3[c0 + q];
         v[q] = sm_a3[c0 + q] * (1.f - h2 * h2);
       }
-      *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, c0, 128)) = tc::pack8(v);
-      *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, c0 + 8, 128)) = tc::pack8(v + 8);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) *reinterpret_cast<uint4*>(sAct + tc::kmajor_off(p, c0 + 8 * k, 128)) = tc::pack8(v + 8 * k);
     }
     sEn[half][p] = e;
   }
@@ -919,13 +921,13 @@ __global__ void __launch_bounds__(256) k_tc_fit(FitTcArgs f) {
   // B1: dE/dG = g1 A1^T (N = 256)
   if (ok) ok = fit_mma(tmem, aH1, 128, aW0, 256, &bar, 1, &bar_w[0], 0, t, f.ctrl, true);
   if (ok) {
-    for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += 16) {
-      float v[16];
-      tc::tmem_ld16(taddr + c0, v);   // warp-collective: every lane loads, valid rows store
+    for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += 32) {
+      float v[32];
+      tc::tmem_ld16x2(taddr + c0, taddr + c0 + 16, v, v + 16);   // warp-collective: every lane loads, valid rows store
       if (valid) {
         float4* dst = reinterpret_cast<float4*>(f.dG + (size_t)atom * 256 + c0);
-        dst[0] = make_float4(v[0], v[1], v[2], v[3]); dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-        dst[2] = make_float4(v[8], v[9], v[10], v[11]); dst[3] = make_float4(v[12], v[13], v[14], v[15]);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) dst[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
       }
     }
   }
