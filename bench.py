@@ -729,7 +729,8 @@ def main():
     reps = 20
     e.compute_forces(ev=False)
     kms = {"pair": time_enqueue(e, stream, 0, reps), "bonded": time_enqueue(e, stream, 2, reps),
-           "verlet": time_enqueue(e, stream, 4, reps), "rebuild": time_enqueue(e, stream, 1, 5)}
+           "verlet": time_enqueue(e, stream, 4, reps), "rebuild": time_enqueue(e, stream, 1, 5),
+           "pair_energy_step": time_enqueue(e, stream, 7, reps)}
     if wl.get("nnp"):
         kms["network"] = time_enqueue(e, stream, 3, reps)
     hbm, bf16, bf16s, src = peaks()

@@ -258,7 +258,8 @@ int nnpe_tc_selftest(int device, int mode, int N, int K, const float* A, const f
 
 /* ---- profiling ------------------------------------------------------------------------
  * Enqueue one kernel class without synchronising (for event timing): 0 pair force, 1 list
- * rebuild, 2 bonded, 3 network term, 4 Verlet, 5 cell-based g(r), 6 list-based g(r). */
+ * rebuild, 2 bonded, 3 network term, 4 Verlet, 5 cell-based g(r), 6 list-based g(r), 7 pair force
+ * with the FP64 energy and virial (an energy step's pair pass). */
 int nnpe_profile_enqueue(nnpe_ctx* ctx, int which);
 /* Number of kernel launches in one plain MD step (the nodes of its CUDA graph). */
 int nnpe_launches_per_step(nnpe_ctx* ctx);

@@ -14,9 +14,6 @@ constexpr float kElectricK = 332.06371f;
 
 struct PairParams {
   const float4* pos;
-  const int* gowner;
-  const int* gshift;
-  GridParams g;
   const uint32_t* list;     // the full list
   const int* ncount;
   // the pruned copy (nullptr: pruning off). The pass reads it, or, when CTRL_PRUNE is set at its
@@ -34,6 +31,11 @@ struct PairParams {
   double* watom;
   int N, cap, ntype, nbin;
   float cutoff, cutsq, r_dr, vc, fc;
+  // energy/virial steps: entries with float rsq >= evgatesq skip the FP64 evaluation. The gate
+  // lies 0.1 % beyond the cutoff, far outside the float/double rsq difference of any image, so
+  // the FP64 test rsq < rc^2 still decides which pairs count.
+  float evgatesq;
+  double rc64, vc64, fc64;   // cutoff, -1/rc and -1/rc^2 in double (pair.cpp:191-193)
   bool accumulate;
   // the network term's pair list, filtered here from the same distances (nullptr: not wanted)
   uint32_t* list6;
@@ -43,45 +45,46 @@ struct PairParams {
   int* ctrl;
 };
 
-// One warp per atom: lanes stride over the atom's list row (coalesced 128-byte reads), gather
-// neighbour positions, and reduce with shuffles; the warp writes the atom's force once (no
-// atomics, deterministic). With list6 set, the entries inside the network cutoff (the same float
-// rsq, the reference's `rsq < cutsq` of pair_nnp.cpp:656) are compacted in list order into the
-// network's pair list on the way, so the list is read once per step.
-// Exact double coordinates of list entry j: a real atom's float position, or its owner's float
-// position plus the float box shift added in double (the image the float list entry rounds).
-__device__ __forceinline__ double3 exact_pos(const PairParams& p, int j) {
-  if (j < p.N) {
-    const float4 x = p.pos[j];
-    return make_double3(x.x, x.y, x.z);
+// 1/sqrt(a) in double with neither a division nor a square root: the single-precision hardware
+// estimate refined by two Newton-Raphson steps for f(y) = 1/y^2 - a, y <- y + y (1 - a y^2) / 2.
+// Each step squares the relative error (times 1.5): below 2^-22 for the estimate, below 2^-43
+// after one step, and at double rounding after the second.
+__device__ __forceinline__ double rsqrt64(double a) {
+  double y = (double)rsqrtf((float)a);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double t = fma(-(a * y), y, 1.0);
+    y = fma(0.5 * y, t, y);
   }
-  const int k = j - p.N;
-  const float4 x = p.pos[p.gowner[k]];
-  float s[3];
-  shift_of(p.g, p.gshift[k], s);
-  return make_double3((double)x.x + (double)s[0], (double)x.y + (double)s[1], (double)x.z + (double)s[2]);
+  return y;
 }
 
 // FP64 pair energy and fpair*rsq of one pair at double separation: the energy/virial reductions of
 // ev steps (pair.cpp:365-410) evaluated in double so that cancellation in the Coulomb sum does not
-// leave FP32 rounding in the total.
+// leave FP32 rounding in the total. 1/r, 1/r^3 and fc/r come from one double 1/sqrt(rsq).
 __device__ __forceinline__ void pair_energy64(const PairParams& p, const float2* tab0, int s, double qq, double rsq,
                                               double* e, double* w) {
-  const double rc = p.cutoff;
+  const double rc = p.rc64;
   if (!(rsq < rc * rc)) return;
-  const double r = sqrt(rsq);
+  const double rinv = rsqrt64(rsq);
+  const double r = rsq * rinv;
   double u = r * (double)p.r_dr - 0.5;
   const int t1 = (int)u;
   const double w2 = u - t1, w1 = 1 - w2;
   const float2 a = tab0[t1], b = tab0[t1 + 1];
   const double slj = c_special_lj[s], sco = s == 3 ? 5.0 / 6.0 : (double)c_special_coul[s];
-  const double vc = -1 / rc, fc = vc / rc;
-  const double fpair = ((double)a.x * w1 + (double)b.x * w2) * slj + qq * (1 / (r * rsq) + fc / r) * sco;
-  const double ue = ((double)a.y * w1 + (double)b.y * w2) * slj + qq * (1 / r + vc + fc * (rc - r)) * sco;
+  const double vc = p.vc64, fc = p.fc64;
+  const double fpair = ((double)a.x * w1 + (double)b.x * w2) * slj + qq * (rinv * rinv * rinv + fc * rinv) * sco;
+  const double ue = ((double)a.y * w1 + (double)b.y * w2) * slj + qq * (rinv + vc + fc * (rc - r)) * sco;
   *e += 0.5 * ue;
   *w += 0.5 * fpair * rsq;
 }
 
+// One warp per atom: lanes stride over the atom's list row (coalesced 128-byte reads), gather
+// neighbour positions, and reduce with shuffles; the warp writes the atom's force once (no
+// atomics, deterministic). With list6 set, the entries inside the network cutoff (the same float
+// rsq, the reference's `rsq < cutsq` of pair_nnp.cpp:656) are compacted in list order into the
+// network's pair list on the way, so the list is read once per step.
 // EXACT=true evaluates fpair with the reference's float sequence (IEEE sqrt and divisions, no
 // contraction), bit-identical per pair. EXACT=false keeps the same cutoff test (so the same pairs
 // interact) but uses rsqrt and fused multiply-adds: ~1 ulp per pair, forces within 1e-6 relative.
@@ -159,9 +162,9 @@ __device__ __forceinline__ void pair_row(const PairParams& p, int i, int lane, b
       }
       fx = fmaf(dx, fpair, fx); fy = fmaf(dy, fpair, fy); fz = fmaf(dz, fpair, fz);
     }
-    if (EV) {
-      const double3 xjd = exact_pos(p, j);
-      const double ddx = (double)xi.x - xjd.x, ddy = (double)xi.y - xjd.y, ddz = (double)xi.z - xjd.z;
+    if (EV && rsq < p.evgatesq) {
+      // the separation of the two float positions the forces use, exact in double
+      const double ddx = (double)xi.x - (double)xj.x, ddy = (double)xi.y - (double)xj.y, ddz = (double)xi.z - (double)xj.z;
       const int tj = (ent >> 27) & 7, s = ent >> 30;
       pair_energy64(p, p.table + (size_t)ptrow[tj] * (p.nbin + 1), s, (double)xi.w * (double)xj.w * 332.06371,
                     ddx * ddx + ddy * ddy + ddz * ddz, &e, &w);
@@ -451,12 +454,13 @@ int pair_enqueue(nnpe_ctx* c, bool ev, bool filter6) {
   const bool pr = prune_in_pair(c);
   p.plist = pr ? c->d_plist : nullptr; p.pcount = pr ? c->d_pcount : nullptr; p.xprune = pr ? c->d_xprune : nullptr;
   p.prunesq = pr ? prune_cutsq(c) : 0.f;
-  p.gowner = c->d_gowner; p.gshift = c->d_gshift; p.g = c->grid;
   p.pairtype = c->d_pairtype; p.frc = c->d_frc; p.eatom = c->d_eatom; p.watom = c->d_watom;
   p.N = N; p.cap = c->cap; p.ntype = c->ntype; p.nbin = c->nbin;
   p.cutoff = c->pair_cutoff; p.cutsq = c->pair_cutoff * c->pair_cutoff;
   p.r_dr = (float)c->nbin / c->pair_cutoff;   // LJTableCoulDSF ctor (pair.cpp:176-177)
   p.vc = -1 / p.cutoff; p.fc = p.vc / p.cutoff;  // pair.cpp:191-193 (erfc disabled)
+  p.rc64 = p.cutoff; p.vc64 = -1 / p.rc64; p.fc64 = p.vc64 / p.rc64;
+  p.evgatesq = p.cutsq * 1.002f;
   p.accumulate = false;
   p.list6 = nullptr; p.n6 = nullptr; p.cap6 = 0; p.cut6sq = 0.f; p.ctrl = c->d_ctrl;
   if (filter6) {

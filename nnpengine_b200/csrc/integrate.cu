@@ -416,6 +416,7 @@ extern "C" int nnpe_profile_enqueue(nnpe_ctx* c, int which) {
     }
     case 5: return c->d_gr_counts ? gr_tally_enqueue(c, 0) : nnpe_fail(c, NNPE_EARG, "no g(r)");
     case 6: return c->d_gr_counts ? gr_tally_enqueue(c, 1) : nnpe_fail(c, NNPE_EARG, "no g(r)");
+    case 7: return pair_enqueue(c, true, pair_filters_list6(c));
   }
   return nnpe_fail(c, NNPE_EARG, "nnpe_profile_enqueue: unknown kernel class");
 }
