@@ -115,7 +115,6 @@ __device__ __forceinline__ void pair_row(const PairParams& p, int i, int lane, b
     e_nx = e_nx2;
     x_nx = k + 32 < n ? __ldg(p.pos + (e_nx & NNPE_J_MASK)) : xi;
     e_nx2 = k + 64 < n ? __ldg(row + k + 64) : 0u;
-    const int j = (int)(ent & NNPE_J_MASK);
     float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
     const float rsq = dx * dx + dy * dy + dz * dz;
     if (out6) {   // warp-uniform

@@ -247,62 +247,92 @@ __global__ void k_ghost_gather(const int* __restrict__ perm, const int* __restri
   }
 }
 
-// NEIGHLIST::build<true> (neighlist.cpp:190-331): one warp per atom walks the stencil rows of
-// its cell, real atoms first then images, and appends accepted candidates in index order.
-// A candidate is accepted without a distance test when its cell carries the no-check bit
-// (NEGH_USE_INNERCUT), else when rsq < (cutoff+skin)^2 in the reference's float sequence.
-__global__ void __launch_bounds__(128) k_build_list(const float4* __restrict__ pos, const int2* __restrict__ info,
+// NEIGHLIST::build<true> (neighlist.cpp:190-331). The atoms of one cell share its stencil rows, so
+// one warp takes a group of up to kBuildGroup atoms of a cell, reads each candidate of the rows
+// (cell, position, type) once, and tests it against every atom of the group. Each atom's row is
+// appended exactly as a warp of its own would: real cells, then image cells, in stencil-row order
+// and index order, ballot-compacted. A candidate is accepted without a distance test when its cell
+// carries the no-check bit (NEGH_USE_INNERCUT; the candidate's cell is read only in rows that have
+// such cells), else when rsq < (cutoff+skin)^2 in the reference's float sequence.
+// kBuildWarpsPerCell warps share a cell's groups (group g goes to warp g mod that); at 6 Å cells
+// (half of cutoff + skin) a cell holds about 22 atoms of water, so its groups usually run at once,
+// and the register cap keeps 8 CTAs per SM.
+constexpr int kBuildGroup = 4;
+constexpr int kBuildWarpsPerCell = 6;
+__global__ void __launch_bounds__(128, 8) k_build_list(const float4* __restrict__ pos, const int2* __restrict__ info,
                                                     const int* __restrict__ cell, const int* __restrict__ cstart,
                                                     const int* __restrict__ cend, const int* __restrict__ gcstart,
                                                     const int* __restrict__ gcend, const int4* __restrict__ rows,
                                                     const int* __restrict__ nrows, int maxrows,
                                                     const int* __restrict__ special, int nmax,
                                                     uint32_t* __restrict__ list, int* __restrict__ ncount,
-                                                    float4* __restrict__ xbuild, int N, int cap, float cutsq,
+                                                    float4* __restrict__ xbuild, int ncell, int cap, float cutsq,
                                                     int* ctrl, bool cond) {
   if (skip(ctrl, cond)) return;
   const int lane = threadIdx.x & 31;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (i >= N) return;
-  const float4 xi = pos[i];
-  const int2 infi = info[i];
-  const int ci = cell[i];
-  const int* spi = special + (info_moltype(infi) * nmax + info_intra(infi)) * nmax;
-  uint32_t* row_out = list + (size_t)i * cap;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int ci = wid / kBuildWarpsPerCell;
+  if (ci >= ncell) return;
+  const int a0 = cstart[ci], a1 = cend[ci];
   const int nr = nrows[ci];
   const int4* R = rows + (size_t)ci * maxrows;
-  int cnt = 0;
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int r = 0; r < nr; ++r) {
-      const int4 row = R[r];
-      const int j0 = pass ? gcstart[row.x] : cstart[row.x];
-      const int j1 = pass ? gcend[row.y] : cend[row.y];
-      for (int base = j0; base < j1; base += 32) {
-        const int j = base + lane;
-        bool ok = false;
-        if (j < j1 && (pass || j != i)) {
-          const int cj = cell[j];
-          if ((row.z >> (cj - row.x)) & 1) ok = true;
-          else {
-            const float4 xj = pos[j];
-            ok = rsq3(fsub(xi.x, xj.x), fsub(xi.y, xj.y), fsub(xi.z, xj.z)) < cutsq;
+  const unsigned below = (1u << lane) - 1;
+  for (int g0 = a0 + (wid % kBuildWarpsPerCell) * kBuildGroup; g0 < a1; g0 += kBuildWarpsPerCell * kBuildGroup) {
+    const int na = min(kBuildGroup, a1 - g0);
+    float xi[kBuildGroup], yi[kBuildGroup], zi[kBuildGroup];
+    int mol[kBuildGroup], spo[kBuildGroup], cnt[kBuildGroup];
+#pragma unroll
+    for (int k = 0; k < kBuildGroup; ++k) {
+      const int i = g0 + min(k, na - 1);
+      const float4 x = pos[i];
+      const int2 inf = info[i];
+      xi[k] = x.x; yi[k] = x.y; zi[k] = x.z;
+      mol[k] = inf.x;
+      spo[k] = (info_moltype(inf) * nmax + info_intra(inf)) * nmax;
+      cnt[k] = 0;
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int r = 0; r < nr; ++r) {
+        const int4 row = R[r];
+        const int j0 = pass ? gcstart[row.x] : cstart[row.x];
+        const int j1 = pass ? gcend[row.y] : cend[row.y];
+        for (int base = j0; base < j1; base += 32) {
+          const int j = base + lane;
+          const bool inr = j < j1;
+          float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+          int2 infj = make_int2(-1, 0);
+          bool nochk = false;
+          if (inr) {
+            if (row.z) nochk = (row.z >> (cell[j] - row.x)) & 1;
+            xj = pos[j];
+            infj = info[j];
+          }
+          const uint32_t ent = (uint32_t)j | ((uint32_t)info_type(infj) << 27);
+#pragma unroll
+          for (int k = 0; k < kBuildGroup; ++k) {
+            if (k < na) {
+              const bool ok = inr && (pass || j != g0 + k) &&
+                              (nochk || rsq3(fsub(xi[k], xj.x), fsub(yi[k], xj.y), fsub(zi[k], xj.z)) < cutsq);
+              const unsigned b = __ballot_sync(0xffffffffu, ok);
+              if (ok) {
+                const int sp = infj.x == mol[k] ? special[spo[k] + info_intra(infj)] : 0;
+                const int idx = cnt[k] + __popc(b & below);
+                if (idx < cap) list[(size_t)(g0 + k) * cap + idx] = ent | ((uint32_t)sp << 30);
+              }
+              cnt[k] += __popc(b);
+            }
           }
         }
-        const unsigned b = __ballot_sync(0xffffffffu, ok);
-        if (ok) {
-          const int2 infj = info[j];
-          const int s = infj.x == infi.x ? spi[info_intra(infj)] : 0;
-          const int idx = cnt + __popc(b & ((1u << lane) - 1));
-          if (idx < cap) row_out[idx] = (uint32_t)j | ((uint32_t)info_type(infj) << 27) | ((uint32_t)s << 30);
-        }
-        cnt += __popc(b);
       }
     }
-  }
-  if (lane == 0) {
-    ncount[i] = min(cnt, cap);
-    xbuild[i] = xi;
-    if (cnt >= cap) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_LIST_OVERFLOW);
+#pragma unroll
+    for (int k = 0; k < kBuildGroup; ++k) {
+      if (k < na && lane == 0) {
+        ncount[g0 + k] = min(cnt[k], cap);
+        xbuild[g0 + k] = make_float4(xi[k], yi[k], zi[k], pos[g0 + k].w);
+        if (cnt[k] >= cap) atomicOr(ctrl + CTRL_ERR, NNPE_DEV_LIST_OVERFLOW);
+      }
+    }
   }
 }
 
@@ -418,9 +448,9 @@ int rebuild_enqueue(nnpe_ctx* c, bool cond) {
                                               c->d_gshift, c->d_pos, c->d_info, c->d_cell, c->d_atom_id, c->d_sorted_of_id,
                                               c->d_mol_rep, c->d_molshift, N, G, g, ctrl, cond);
   const float cs = c->pair_cutoff + c->skin;
-  k_build_list<<<nblocks((long)N * 32, 128), 128, 0, st>>>(
+  k_build_list<<<nblocks((long)NG * kBuildWarpsPerCell * 32, 128), 128, 0, st>>>(
       c->d_pos, c->d_info, c->d_cell, c->d_cstart, c->d_cend, c->d_gcstart, c->d_gcend, c->st_pair.rows, c->st_pair.nrows,
-      c->st_pair.maxrows, c->d_special, c->nmax, c->d_list, c->d_ncount, c->d_xbuild, N, c->cap, cs * cs, ctrl, cond);
+      c->st_pair.maxrows, c->d_special, c->nmax, c->d_list, c->d_ncount, c->d_xbuild, NG, c->cap, cs * cs, ctrl, cond);
   NNPE_CHECK_LAUNCH(c);
   return 0;
 }
