@@ -105,6 +105,8 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.first = 0   # index of the last sample taken before the timed region
+        self.bracketed = False
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -115,6 +117,13 @@ class ClockSampler:
                                           "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a few hundred ms to start: wait for its first sample so that sampling
+            # is running when the timed region begins (a region of a few tens of ms can otherwise
+            # end before the first sample)
+            t_end = time.time() + 5
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.first = max(len(self.lines) - 1, 0)
         except FileNotFoundError:
             self.proc = None
         return self
@@ -125,6 +134,14 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            # one sample after the region: with the last one before it, a region shorter than the
+            # 50 ms interval is still bracketed by samples taken next to it under the same load
+            n = len(self.lines)
+            if n - self.first < 3:
+                self.bracketed = True
+                t_end = time.time() + 1
+                while len(self.lines) <= n and time.time() < t_end and self.proc.poll() is None:
+                    time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -134,7 +151,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        for l in self.lines[self.first:]:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
@@ -146,8 +163,11 @@ class ClockSampler:
             for n, v in zip(names, f[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+               "samples": len(sm)}
+        if self.bracketed:
+            out["note"] = "timed region shorter than a few 50 ms intervals: the samples include the last one before it and the first one after it"
+        return out
 
 
 MIX_SIGMA, MIX_EPS = (3.0, 3.4), (0.15, 0.25)
