@@ -32,8 +32,8 @@ struct PairParams {
   int N, cap, ntype, nbin;
   float cutoff, cutsq, r_dr, vc, fc;
   // energy/virial steps: entries with float rsq >= evgatesq skip the FP64 evaluation. The gate
-  // lies 0.1 % beyond the cutoff, far outside the float/double rsq difference of any image, so
-  // the FP64 test rsq < rc^2 still decides which pairs count.
+  // lies 0.2 % beyond rc^2, far outside the few-ulp rounding of the float rsq, so the FP64 test
+  // rsq < rc^2 on the same two positions still decides which pairs count.
   float evgatesq;
   double rc64, vc64, fc64;   // cutoff, -1/rc and -1/rc^2 in double (pair.cpp:191-193)
   bool accumulate;
