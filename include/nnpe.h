@@ -164,6 +164,19 @@ int nnpe_list_info(nnpe_ctx* ctx, int* nghost, int64_t* nentries, int* nbuild, i
 /* Full list as records (atom id i, atom id j, image code, special class); image code
  * (sx+1)*9+(sy+1)*3+(sz+1) of the ghost shift, 13 for a real atom. cap = record capacity. */
 int nnpe_list_get(nnpe_ctx* ctx, int64_t cap, int* rec, int64_t* n);
+/* ENVIRON::verify_grid (environ.cpp:638-683), the cell sort's invariants: real atoms fill the
+ * cells in order from index 0 and images from index natom, cell ranges are contiguous, and every
+ * entry's stored cell is the cell of its position in the reference's float arithmetic. Where the
+ * reference ends the program, these return NNPE_ERANGE. nnpe_verify_grid checks the context's
+ * own sort (host copies; meaningful right after nnpe_list_build, as positions move between
+ * builds). nnpe_verify_grid_arrays checks host arrays: cstart/cend/gcstart/gcend [num_gx^3],
+ * cell [natom+nimage], pos4 [natom+nimage][4]; on a violation *bad is the cell or entry index
+ * and *what its kind (1 bounds, 2 contiguity, 3 reversed range, 4 stored cell, 5 position's
+ * cell). */
+int nnpe_verify_grid(nnpe_ctx* ctx);
+int nnpe_verify_grid_arrays(int natom, int nimage, int num_gx, float g_offset, float g_rdx, const int* cstart,
+                            const int* cend, const int* gcstart, const int* gcend, const int* cell,
+                            const float* pos4, int64_t* bad, int* what);
 /* Dynamic pruning of the list (no counterpart in the reference, which evaluates every list entry;
  * the pairs that interact are the same). With delta > 0 (and below the skin) the pair and network
  * kernels read a copy of the list that keeps the entries within max(pair, network cutoff) + delta;

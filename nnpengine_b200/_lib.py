@@ -62,6 +62,9 @@ _SIGS = {
     "nnpe_set_prune": (C.c_int, [_vp, C.c_double]),
     "nnpe_prune_info": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
     "nnpe_list_get": (C.c_int, [_vp, C.c_int64, _i32p, C.POINTER(C.c_int64)]),
+    "nnpe_verify_grid": (C.c_int, [_vp]),
+    "nnpe_verify_grid_arrays": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _i32p, _i32p, _i32p, _i32p,
+                                          _i32p, _f32p, C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     "nnpe_compute_forces": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nnpe_get_forces": (C.c_int, [_vp, C.c_int, _f32p]),
     "nnpe_force_step": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),

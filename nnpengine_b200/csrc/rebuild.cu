@@ -4,6 +4,8 @@
 // Every kernel takes the device rebuild flag and returns at once when it is clear, so that one
 // step is a fixed launch sequence (capturable in a CUDA graph) and the decision "is the list
 // still valid" (NEIGHLIST::isvalid, neighlist.cpp:178-187) never round-trips to the host.
+#include <algorithm>
+
 #include "internal.cuh"
 
 namespace {
@@ -544,5 +546,73 @@ extern "C" int nnpe_ghost_update(nnpe_ctx* c) {
                                                                c->grid, c->d_ctrl);
   prune_enqueue(c);
   NNPE_CHECK_LAUNCH(c);
+  return NNPE_OK;
+}
+
+// ENVIRON::verify_grid (environ.cpp:638-683) on host copies of a cell sort: the real atoms fill
+// the cells in cell order from index 0 and the images from index natom, each cell's range starts
+// where the previous one ends, and every entry's stored cell is both the cell whose range holds it
+// and the cell of its position in the reference's float arithmetic ((int)((g_offset + x) * g_rdx)
+// per axis, environ.cpp:252-260). Returns NNPE_ERANGE at the first violation, with its cell or
+// entry index in *bad and a code in *what (1 bounds, 2 contiguity, 3 reversed range, 4 stored cell,
+// 5 position's cell).
+extern "C" int nnpe_verify_grid_arrays(int natom, int nimage, int num_gx, float g_offset, float g_rdx,
+                                       const int* cstart, const int* cend, const int* gcstart, const int* gcend,
+                                       const int* cell, const float* pos4, int64_t* bad, int* what) {
+  if (natom <= 0 || nimage < 0 || num_gx <= 0 || !cstart || !cend || !gcstart || !gcend || !cell || !pos4)
+    return NNPE_EARG;
+  const int NG = num_gx * num_gx * num_gx, ntot = natom + nimage;
+  auto fail = [&](int code, int64_t idx) {
+    if (bad) *bad = idx;
+    if (what) *what = code;
+    return (int)NNPE_ERANGE;
+  };
+  auto axis = [&](float x) {
+    const float s = g_offset + x;   // rounded, then multiplied and rounded: the device's fadd, fmul
+    return (int)(s * g_rdx);
+  };
+  if (cstart[0] != 0 || gcstart[0] != natom || cend[NG - 1] != natom || gcend[NG - 1] != ntot) return fail(1, 0);
+  for (int i = 1; i < NG; ++i)
+    if (cstart[i] != cend[i - 1] || gcstart[i] != gcend[i - 1]) return fail(2, i);
+  for (int i = 0; i < NG; ++i) {
+    for (int pass = 0; pass < 2; ++pass) {
+      const int j0 = pass ? gcstart[i] : cstart[i], j1 = pass ? gcend[i] : cend[i];
+      if (j0 > j1 || j0 < 0 || j1 > ntot) return fail(3, i);
+      for (int j = j0; j < j1; ++j) {
+        if (cell[j] != i) return fail(4, j);
+        const float* x = pos4 + 4 * (size_t)j;
+        if (axis(x[0]) * num_gx * num_gx + axis(x[1]) * num_gx + axis(x[2]) != i) return fail(5, j);
+      }
+    }
+  }
+  if (bad) *bad = -1;
+  if (what) *what = 0;
+  return NNPE_OK;
+}
+
+// The same check on the context's own cell sort (copied from the device; synchronises its stream).
+// Positions move between list builds, so it is meaningful right after a build (nnpe_list_build).
+extern "C" int nnpe_verify_grid(nnpe_ctx* c) {
+  if (!c || !c->have_setup) return nnpe_fail(c, NNPE_EARG, "nnpe_verify_grid: not set up");
+  if (int rc = sync_errors(c)) return rc;
+  const int N = c->natom, NG = c->grid.num_grid;
+  NNPE_CUDA(c, cudaMemcpyAsync(c->h_ctrl, c->d_ctrl, sizeof(int) * CTRL_WORDS, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int ng = std::min(c->h_ctrl[CTRL_NGHOST], c->Gcap), ntot = N + ng;
+  std::vector<int> cs(NG), ce(NG), gs(NG), ge(NG), cell(ntot);
+  std::vector<float4> pos(ntot);
+  NNPE_CUDA(c, cudaMemcpyAsync(cs.data(), c->d_cstart, sizeof(int) * NG, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(ce.data(), c->d_cend, sizeof(int) * NG, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(gs.data(), c->d_gcstart, sizeof(int) * NG, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(ge.data(), c->d_gcend, sizeof(int) * NG, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(cell.data(), c->d_cell, sizeof(int) * ntot, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaMemcpyAsync(pos.data(), c->d_pos, sizeof(float4) * ntot, cudaMemcpyDeviceToHost, c->stream));
+  NNPE_CUDA(c, cudaStreamSynchronize(c->stream));
+  int64_t bad = -1;
+  int what = 0;
+  const int rc = nnpe_verify_grid_arrays(N, ng, c->grid.num_gx, c->grid.g_offset, c->grid.g_rdx, cs.data(), ce.data(),
+                                         gs.data(), ge.data(), cell.data(), reinterpret_cast<const float*>(pos.data()),
+                                         &bad, &what);
+  if (rc) return nnpe_fail(c, rc, "nnpe_verify_grid: violation " + std::to_string(what) + " at " + std::to_string(bad));
   return NNPE_OK;
 }

@@ -238,6 +238,10 @@ class Engine:
         self._ok(self.lib.nnpe_prune_info(self.h, C.byref(d), C.byref(a), C.byref(n), C.byref(ne)))
         return dict(delta=d.value, active=bool(a.value), nprune=n.value, entries=ne.value)
 
+    def verify_grid(self) -> None:
+        """ENVIRON::verify_grid on the device's cell sort (raises on a violation)."""
+        self._ok(self.lib.nnpe_verify_grid(self.h))
+
     def list_records(self) -> np.ndarray:
         n = self.list_info()["entries"]
         rec = np.zeros(4 * max(n, 1), np.int32)
