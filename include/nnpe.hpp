@@ -73,6 +73,9 @@ class ENVIRON {
   static void sort() {}
   static void tidyup_ghost() {}
   static void sort_ghost() {}
+  /* verify_grid (environ.cpp:638-683): the cell sort's invariants on the device's sort; a
+   * violation ends the program as the reference's END_PROGRAM("verify_grid fail") does */
+  static void verify_grid() { check(nnpe_verify_grid(ctx), "verify_grid fail", ctx); }
   static void dump(const char* xyzfile, bool append = false) {
     std::vector<float> x((size_t)natom * 3);
     std::vector<int> typ(natom);
